@@ -1,0 +1,361 @@
+"""ctypes binding of include/cr_gpu.h (libcr_b200.so).
+
+The record layouts below are numpy dtypes that match the C structs byte for byte (and
+therefore CPU-Renderer's cr::Triangle, cr::Ray, cr::Hit and Bvh::Node). The binding raises
+RuntimeError with the library's message on any non-zero status; there is no fallback path:
+if libcr_b200.so is missing, importing this module fails.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcr_b200.so")
+
+vertex_dtype = np.dtype([("position", "<f4", 3), ("normal", "<f4", 3), ("tangent", "<f4", 4), ("uv", "<f4", (2, 2))])
+triangle_dtype = np.dtype([("v", vertex_dtype, 3), ("material", "<u4"), ("geometric_normal", "<f4", 3), ("area", "<f4")])
+ray_dtype = np.dtype([("origin", "<f4", 3), ("direction", "<f4", 3), ("tmin", "<f4"), ("tmax", "<f4"), ("origin_low", "<f4", 3)])
+hit_dtype = np.dtype([("t", "<f8"), ("u", "<f8"), ("v", "<f8"), ("triangle", "<u4"), ("reserved", "<u4")])
+node_dtype = np.dtype([("lo", "<f4", 3), ("hi", "<f4", 3), ("first", "<u4"), ("count", "<u4")])
+slot_dtype = np.dtype([("texture", "<i4"), ("texcoord", "<i4"), ("offset", "<f4", 2), ("scale", "<f4", 2), ("rotation", "<f4")])
+material_dtype = np.dtype([
+    ("base_color", "<f4", 4), ("metallic", "<f4"), ("roughness", "<f4"), ("emission", "<f4", 3),
+    ("transmission", "<f4"), ("ior", "<f4"), ("thickness", "<f4"), ("attenuation_distance", "<f4"),
+    ("attenuation_color", "<f4", 3), ("double_sided", "<i4"), ("alpha_mode", "<i4"), ("alpha_cutoff", "<f4"),
+    ("normal_scale", "<f4"), ("base_color_texture", slot_dtype), ("metallic_roughness_texture", slot_dtype),
+    ("normal_texture", slot_dtype), ("emissive_texture", slot_dtype), ("transmission_texture", slot_dtype)])
+light_dtype = np.dtype([("type", "<i4"), ("position", "<f4", 3), ("direction", "<f4", 3), ("color", "<f4", 3),
+                        ("intensity", "<f4"), ("range", "<f4"), ("inner_cone", "<f4"), ("outer_cone", "<f4")])
+texture_dtype = np.dtype([("image", "<i4"), ("wrap_s", "<i4"), ("wrap_t", "<i4"), ("linear", "<i4")])
+
+assert triangle_dtype.itemsize == 188 and ray_dtype.itemsize == 44 and hit_dtype.itemsize == 32
+assert node_dtype.itemsize == 32 and material_dtype.itemsize == 220 and light_dtype.itemsize == 56
+
+WRAP_REPEAT, WRAP_CLAMP, WRAP_MIRROR = 0, 1, 2
+ALPHA_OPAQUE, ALPHA_MASK = 0, 1
+LIGHT_POINT, LIGHT_DIRECTIONAL, LIGHT_SPOT = 0, 1, 2
+INF = float("inf")
+NO_TRIANGLE = 0xFFFFFFFF
+
+
+def new_materials(n):
+    """Materials with cr::Material's defaults (scene.h:187-199)."""
+    m = np.zeros(n, material_dtype)
+    m["base_color"] = 1.0
+    m["metallic"] = 1.0
+    m["roughness"] = 1.0
+    m["ior"] = 1.5
+    m["attenuation_distance"] = INF
+    m["attenuation_color"] = 1.0
+    m["alpha_cutoff"] = 0.5
+    m["normal_scale"] = 1.0
+    for k in ("base_color_texture", "metallic_roughness_texture", "normal_texture", "emissive_texture", "transmission_texture"):
+        m[k]["texture"] = -1
+        m[k]["scale"] = 1.0
+    return m
+
+
+def new_triangles(n):
+    """Triangles with cr::Vertex defaults (tangent w = 1)."""
+    t = np.zeros(n, triangle_dtype)
+    t["v"]["tangent"][..., 3] = 1.0
+    return t
+
+
+def new_lights(n):
+    l = np.zeros(n, light_dtype)
+    l["direction"] = (0, 0, -1)
+    l["color"] = 1.0
+    l["intensity"] = 1.0
+    l["range"] = INF
+    l["outer_cone"] = np.float32(np.pi / 4)
+    return l
+
+
+class Camera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("forward", C.c_float * 3), ("right", C.c_float * 3), ("up", C.c_float * 3),
+                ("yfov", C.c_float), ("aspect", C.c_float), ("near_clip", C.c_float), ("far_clip", C.c_float)]
+
+    @classmethod
+    def make(cls, position=(0, 0, 0), forward=(0, 0, -1), right=(1, 0, 0), up=(0, 1, 0), yfov=np.pi / 4,
+             aspect=0.0, near_clip=0.01, far_clip=INF):
+        """cr::Camera defaults (scene.h:202-207)."""
+        c = cls()
+        c.position[:] = [float(x) for x in position]
+        c.forward[:] = [float(x) for x in forward]
+        c.right[:] = [float(x) for x in right]
+        c.up[:] = [float(x) for x in up]
+        c.yfov, c.aspect, c.near_clip, c.far_clip = float(np.float32(yfov)), aspect, near_clip, far_clip
+        return c
+
+
+class Options(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("samples", C.c_int32), ("bounces", C.c_int32),
+                ("threads", C.c_int32), ("seed", C.c_uint64), ("next_event_estimation", C.c_int32),
+                ("russian_roulette", C.c_int32)]
+
+    @classmethod
+    def make(cls, width=960, height=540, samples=32, bounces=8, threads=0, seed=42, nee=True, rr=True):
+        """cr::RenderOptions defaults (render.h:31-39)."""
+        return cls(width, height, samples, bounces, threads, seed, int(nee), int(rr))
+
+
+class Stats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("device_ms", C.c_double), ("extend_ms", C.c_double),
+                ("shadow_ms", C.c_double), ("shade_ms", C.c_double), ("workers", C.c_int32), ("waves", C.c_int32),
+                ("camera_samples", C.c_uint64), ("boundary_retries", C.c_uint64), ("extend_rays", C.c_uint64),
+                ("shadow_rays", C.c_uint64), ("kernel_launches", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(C.Structure):
+    _fields_ = [("exact_traversal", C.c_int32), ("env_alias", C.c_int32), ("paths_per_wave", C.c_int32),
+                ("block_size", C.c_int32), ("use_graphs", C.c_int32), ("time_phases", C.c_int32)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("triangles", C.c_void_p), ("triangle_count", C.c_uint64), ("materials", C.c_void_p),
+                ("material_count", C.c_uint32), ("lights", C.c_void_p), ("light_count", C.c_uint32),
+                ("images", C.c_void_p), ("image_count", C.c_uint32), ("textures", C.c_void_p),
+                ("texture_count", C.c_uint32), ("bvh_nodes", C.c_void_p), ("bvh_node_count", C.c_uint64),
+                ("bvh_indices", C.c_void_p), ("bvh_index_count", C.c_uint64)]
+
+
+class Image(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("pixels", C.c_void_p)]
+
+
+class EnvDesc(C.Structure):
+    _fields_ = [("constant", C.c_float * 3), ("pixels", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32),
+                ("rotation_radians", C.c_float), ("intensity", C.c_float), ("cdf", C.c_void_p)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_uint64, C.c_uint64, C.c_double, C.c_void_p)
+
+
+def _ptr(a):
+    return None if a is None or len(a) == 0 else a.ctypes.data
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libcr_b200.so is not built (run cpu-renderer_b200/build.py): " + LIB_PATH)
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    sig = {
+        "cr_gpu_abi_version": (C.c_int, []),
+        "cr_gpu_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+        "cr_gpu_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+        "cr_options_validate": (C.c_int, [C.POINTER(Options)]),
+        "cr_scene_finalize": (C.c_int, [P, C.POINTER(C.c_uint64), P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, C.c_char_p, C.c_size_t]),
+        "cr_bvh_build": (C.c_int, [P, C.c_uint64, P, C.POINTER(C.c_uint64), P]),
+        "cr_environment_rotation": (C.c_float, [C.c_float]),
+        "cr_gpu_scene_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(EnvDesc), C.c_int, C.POINTER(P)]),
+        "cr_gpu_scene_destroy": (C.c_int, [P]),
+        "cr_gpu_scene_bytes": (C.c_int, [P, C.POINTER(C.c_uint64)]),
+        "cr_gpu_intersect": (C.c_int, [P, P, C.c_uint64, C.c_int, C.c_uint32, P, P, C.POINTER(Tuning)]),
+        "cr_gpu_camera_rays": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.c_uint32, P]),
+        "cr_gpu_render": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), PROGRESS_FN, P, P, C.POINTER(Stats), C.POINTER(Tuning)]),
+        "cr_gpu_render_resident": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.POINTER(Stats), C.POINTER(Tuning), P]),
+        "cr_gpu_film_download": (C.c_int, [P, P, C.c_uint64]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    return lib
+
+
+lib = _load()
+
+
+class CrError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+def last_error():
+    buf = C.create_string_buffer(4096)
+    lib.cr_gpu_last_error(buf, len(buf))
+    return buf.value.decode()
+
+
+def check(status):
+    if status != 0:
+        raise CrError(status, last_error())
+
+
+def device_count():
+    n = C.c_int(0)
+    lib.cr_gpu_device_count(C.byref(n))
+    return n.value
+
+
+def validate_options(options):
+    check(lib.cr_options_validate(C.byref(options)))
+
+
+def environment_rotation(degrees):
+    return lib.cr_environment_rotation(float(degrees))
+
+
+def finalize(triangles, materials, images=(), textures=None):
+    """Scene::finalize restated (returns the compacted array and the warnings)."""
+    t = np.ascontiguousarray(triangles, dtype=triangle_dtype).copy()
+    count = C.c_uint64(len(t))
+    img, tex = _images(images), _textures(textures)
+    buf = C.create_string_buffer(8192)
+    check(lib.cr_scene_finalize(_ptr(t), C.byref(count), _ptr(materials), len(materials),
+                                C.cast(img, C.c_void_p) if img else None, len(images),
+                                _ptr(tex), 0 if tex is None else len(tex), buf, len(buf)))
+    w = buf.value.decode()
+    return t[:count.value].copy(), (w.split("\n") if w else [])
+
+
+def build_bvh(triangles):
+    t = np.ascontiguousarray(triangles, dtype=triangle_dtype)
+    n = len(t)
+    nodes = np.zeros(max(1, 2 * n - 1), node_dtype)
+    idx = np.zeros(max(1, n), np.uint32)
+    count = C.c_uint64(0)
+    check(lib.cr_bvh_build(_ptr(t), n, nodes.ctypes.data, C.byref(count), idx.ctypes.data))
+    return nodes[:count.value].copy(), idx[:n].copy()
+
+
+def _images(images):
+    if not images:
+        return None
+    arr = (Image * len(images))()
+    for i, im in enumerate(images):
+        im = np.ascontiguousarray(im, dtype=np.float32)
+        arr[i] = Image(im.shape[1], im.shape[0], im.ctypes.data)
+    arr._keep = images
+    return arr
+
+
+def _textures(textures):
+    if textures is None or len(textures) == 0:
+        return None
+    return np.ascontiguousarray(textures, dtype=texture_dtype)
+
+
+def env_desc(constant=(0, 0, 0), image=None, rotation_degrees=0.0, intensity=1.0):
+    """cr::Environment: a constant radiance, or an RGBA float32 (H, W, 4) equirect image."""
+    e = EnvDesc()
+    e.constant[:] = [float(x) for x in constant]
+    e.intensity = float(intensity)
+    e.rotation_radians = environment_rotation(rotation_degrees)
+    if image is not None:
+        image = np.ascontiguousarray(image, dtype=np.float32)
+        assert image.ndim == 3 and image.shape[2] == 4
+        e.pixels = image.ctypes.data
+        e.height, e.width = image.shape[0], image.shape[1]
+        e._keep = image
+    return e
+
+
+class GpuScene:
+    """A device-resident scene (cr_gpu_scene)."""
+
+    def __init__(self, triangles, materials, lights=None, images=(), textures=None, env=None, bvh=None, device=0):
+        self._arrays = []
+        t = np.ascontiguousarray(triangles, dtype=triangle_dtype)
+        m = np.ascontiguousarray(materials, dtype=material_dtype)
+        l = np.ascontiguousarray(lights if lights is not None else np.zeros(0, light_dtype), dtype=light_dtype)
+        img = _images(images)
+        tex = _textures(textures)
+        d = SceneDesc()
+        d.triangles, d.triangle_count = _ptr(t), len(t)
+        d.materials, d.material_count = _ptr(m), len(m)
+        d.lights, d.light_count = _ptr(l), len(l)
+        d.images, d.image_count = (C.cast(img, C.c_void_p).value if img else None), len(images)
+        d.textures, d.texture_count = _ptr(tex), (0 if tex is None else len(tex))
+        if bvh is not None:
+            nodes, idx = bvh
+            nodes = np.ascontiguousarray(nodes, dtype=node_dtype)
+            idx = np.ascontiguousarray(idx, dtype=np.uint32)
+            d.bvh_nodes, d.bvh_node_count = _ptr(nodes), len(nodes)
+            d.bvh_indices, d.bvh_index_count = _ptr(idx), len(idx)
+            self._arrays += [nodes, idx]
+        self._arrays += [t, m, l, img, tex]
+        e = env if env is not None else env_desc()
+        h = C.c_void_p()
+        check(lib.cr_gpu_scene_create(C.byref(d), C.byref(e), device, C.byref(h)))
+        self.handle = h
+        self.triangle_count = len(t)
+
+    def close(self):
+        if self.handle:
+            lib.cr_gpu_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bytes(self):
+        b = C.c_uint64(0)
+        check(lib.cr_gpu_scene_bytes(self.handle, C.byref(b)))
+        return b.value
+
+    def intersect(self, rays, any_hit=False, ignore=NO_TRIANGLE, hits=None, tuning=None):
+        """Bvh::intersect over a batch; returns (found bool array, hits)."""
+        rays = np.ascontiguousarray(rays, dtype=ray_dtype)
+        n = len(rays)
+        if hits is None:
+            hits = np.zeros(n, hit_dtype)
+            hits["t"] = INF
+        hits = np.ascontiguousarray(hits, dtype=hit_dtype).copy()
+        found = np.zeros(n, np.uint8)
+        check(lib.cr_gpu_intersect(self.handle, _ptr(rays), n, int(any_hit), ignore, _ptr(hits), _ptr(found),
+                                   C.byref(tuning) if tuning else None))
+        return found.astype(bool), hits
+
+    def camera_rays(self, camera, options, sample):
+        out = np.zeros(options.width * options.height, ray_dtype)
+        check(lib.cr_gpu_camera_rays(self.handle, C.byref(camera), C.byref(options), sample, out.ctypes.data))
+        return out
+
+    def render(self, camera, options, progress=None, tuning=None):
+        """cr::render: returns (film float32 (H, W, 3), stats dict)."""
+        film = np.zeros((options.height, options.width, 3), np.float32)
+        stats = Stats()
+        cb = PROGRESS_FN(lambda a, b, s, u: progress(a, b, s)) if progress else PROGRESS_FN(0)
+        check(lib.cr_gpu_render(self.handle, C.byref(camera), C.byref(options), cb, None, film.ctypes.data,
+                                C.byref(stats), C.byref(tuning) if tuning else None))
+        return film, stats.as_dict()
+
+    def render_resident(self, camera, options, tuning=None, per_sample=False):
+        """Film stays on the device; optionally returns every sample's radiance
+        (samples, H, W, 3)."""
+        stats = Stats()
+        ps = None
+        if per_sample:
+            ps = np.zeros((options.samples, options.height, options.width, 3), np.float32)
+        check(lib.cr_gpu_render_resident(self.handle, C.byref(camera), C.byref(options), C.byref(stats),
+                                         C.byref(tuning) if tuning else None, None if ps is None else ps.ctypes.data))
+        return stats.as_dict(), ps
+
+    def film(self, width, height):
+        out = np.zeros((height, width, 3), np.float32)
+        check(lib.cr_gpu_film_download(self.handle, out.ctypes.data, out.size))
+        return out
+
+
+def rel_mse(x, ref, eps=1e-2):
+    """Relative MSE: mean over pixels and channels of (x - r)^2 / (r^2 + eps)."""
+    x = np.asarray(x, np.float64)
+    r = np.asarray(ref, np.float64)
+    return float(np.mean((x - r) ** 2 / (r ** 2 + eps)))
+
+
+def relative_l1(x, ref):
+    """tests/image_metrics.cpp's score: sum |a - b| / sum a over RGB."""
+    x = np.asarray(x, np.float64)
+    r = np.asarray(ref, np.float64)
+    return float(np.abs(x - r).sum() / max(1e-12, r.sum()))

@@ -1,0 +1,64 @@
+// Host-side preparation shared by the C ABI (cr_host.cpp) and the device driver
+// (cr_render.cu). Everything here runs on the CPU once per scene or per render.
+#pragma once
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "cr_gpu.h"
+#include "cr_internal.h"
+
+namespace crh {
+
+// Typed failures carry the cr_status they map to, and the reference's message text.
+struct Error : std::runtime_error {
+    cr_status status;
+    Error(cr_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+cr_status set_last_error(cr_status status, const std::string& message);
+
+void validate_options(const cr_render_options& o);                           // render.cpp:97-104
+
+// Scene::finalize (geometry.cpp:296-397) on a triangle vector.
+void finalize(std::vector<cr_triangle>& triangles, const cr_material* materials, uint32_t materialCount,
+              const cr_image* images, uint32_t imageCount, const cr_texture* textures, uint32_t textureCount,
+              std::vector<std::string>& warnings);
+
+// Bvh::build (geometry.cpp:463-550).
+void build_bvh(const cr_triangle* triangles, uint64_t count, std::vector<cr_bvh_node>& nodes,
+               std::vector<uint32_t>& indices);
+
+// Environment tables (render.cpp:12-42, 67-94).
+struct EnvTables {
+    bool hasImage = false;
+    float constant[3] = {0, 0, 0};
+    int width = 0, height = 0;
+    float rotation = 0, intensity = 1;
+    double integral = 0, weightSum = 0;
+    std::vector<double> cdf;
+    std::vector<float> pdf;       // per texel density
+    std::vector<float> rowCos;    // cos(pi*y/H) for y = 0..H
+    std::vector<uint32_t> coarse; // bracket table for the CDF search
+    std::vector<float> aliasProb;
+    std::vector<uint32_t> aliasIndex;
+};
+void build_environment(const cr_environment_desc& e, EnvTables& out);
+
+// Lights (render.cpp:131-160).
+struct LightTables {
+    std::vector<crg::LightEntry> entries;
+    std::vector<float> triangleProbability;
+    float environmentProbability = 0;
+};
+void build_lights(const cr_triangle* triangles, uint64_t count, const cr_material* materials,
+                  const cr_punctual_light* lights, uint32_t lightCount, double envIntegral, LightTables& out);
+
+// Camera::generate's per-render part (geometry.cpp:214-224). Throws Error with the
+// reference's invalid_argument text when the camera cannot produce rays.
+void camera_setup(const cr_camera& c, int width, int height, crg::DevCamera& out);
+
+// Per-sample failure text, "Pixel (x,y), sample s: <cause>" (render.cpp:437-438).
+std::string sample_error_message(const crg::DevError& e);
+
+}  // namespace crh

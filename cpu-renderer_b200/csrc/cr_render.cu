@@ -1,0 +1,1107 @@
+// Wavefront path tracer for sm_100a: kernels and the host driver behind include/cr_gpu.h.
+//
+// One render (cr::render, render.cpp:352-456) is a sequence of sample waves. A wave holds
+// a block of consecutive sample indices for a range of pixels, one path slot per
+// (pixel, sample). Per bounce it runs:
+//
+//   k_extend  closest hit for the live queue            (Bvh::intersect, geometry.cpp:554)
+//   k_shade   one trace() iteration per path            (render.cpp:240-344)
+//             -> next live queue, shadow queue (warp-ballot compaction)
+//   k_shadow  any hit for the shadow queue; unoccluded contributions are added
+//
+// The per-path state machine keeps the reference's order of random draws and radiance
+// sums, so each camera sample consumes the same SplitMix stream as on the CPU. After a
+// wave, k_accumulate adds every pixel's samples in index order into FP64 sums (render.cpp:
+// 388-415), so the film does not depend on scheduling. Precision replay (render.cpp:403-412)
+// resets the failing path to its camera ray with split origins and runs it again.
+#include "cr_shade.cuh"
+#include "cr_host.h"
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace crg {
+
+struct WaveInfo {
+    uint32_t pixel0, npix, sample0, nsamp, paths;
+};
+
+enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatWords = 4 };
+
+CR_D uint64_t errorKey(const RenderParams& P, uint32_t pixel, uint32_t sample) {
+    const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
+    const uint64_t tilesX = (static_cast<uint64_t>(P.width) + 15) / 16;
+    const uint64_t rank = ((y / 16) * tilesX + x / 16) * 256 + (y % 16) * 16 + (x % 16);
+    return (rank << 21) | sample;
+}
+
+// Error sink: the smallest key is kept for the report; when detail is set (single-sample
+// re-run), the full record is written there.
+struct ErrSink {
+    unsigned long long* minKey;
+    DevError* detail;
+};
+CR_D void raise(const ErrSink& E, const RenderParams& P, uint32_t pixel, uint32_t sample, int code) {
+    atomicMin(E.minKey, static_cast<unsigned long long>(errorKey(P, pixel, sample)));
+    if (E.detail) {
+        E.detail->code = code;
+        E.detail->x = static_cast<int32_t>(pixel % static_cast<uint32_t>(P.width));
+        E.detail->y = static_cast<int32_t>(pixel / static_cast<uint32_t>(P.width));
+        E.detail->sample = static_cast<int32_t>(sample);
+        E.detail->key = errorKey(P, pixel, sample);
+    }
+}
+
+// All 32 lanes call this together; lanes with pred append value to the queue.
+CR_D void warpPush(uint32_t* queue, uint32_t* counter, bool pred, uint32_t value) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) queue[base + __popc(mask & ((1u << lane) - 1u))] = value;
+}
+
+CR_D float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// render.cpp:396-401 plus trace()'s initial state (render.cpp:235-239).
+CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t slot, uint32_t pixel,
+                   uint32_t sample, bool precise, const ErrSink& E) {
+    Rng rng(sampleSeed(P.seed, pixel, sample));
+    const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
+    const float dx = rng.uniform(), dy = rng.uniform();
+    TRay ray;
+    if (!cameraRay(P.camera, P.width, P.height, static_cast<float>(x) + dx, static_cast<float>(y) + dy, ray)) {
+        raise(E, P, pixel, sample, kErrUnrepresentableCameraRay);
+        return false;
+    }
+    st.ray_o[slot] = f4(ray.o, ray.tmin);
+    st.ray_d[slot] = f4(ray.d, ray.tmax);
+    st.ray_lo[slot] = make_float4(0, 0, 0, 0);
+    st.thr[slot] = make_float4(1, 1, 1, 1);          // throughput 1, etaScale 1
+    st.rad[slot] = make_float4(0, 0, 0, 0);          // radiance 0, lastPdf 0
+    st.last_pos[slot] = make_float4(0, 0, 0, 0);
+    st.absorb[slot] = make_float4(0, 0, 0, __int_as_float(-1));  // medium -1
+    st.flags[slot] = kPathLastDelta | (precise ? kPathPrecise : 0u);
+    st.rng[slot] = rng.state;
+    st.prev_tri[slot] = kNoTriangle;
+    st.pixel[slot] = pixel;
+    st.sample[slot] = sample;
+    st.depth[slot] = 0;
+    return true;
+}
+
+CR_D TRay loadRay(const PathSoA& st, uint32_t path, uint32_t flags) {
+    const float4 o = st.ray_o[path], d = st.ray_d[path];
+    TRay r;
+    r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w;
+    r.olow = (flags & kPathPrecise) ? v3(st.ray_lo[path]) : V3{};
+    return r;
+}
+
+// Ends a path: the reference's final radiance check (render.cpp:346), then the sample output.
+CR_D void finishPath(const RenderParams& P, const PathSoA& st, uint32_t path, V3 R, const ErrSink& E) {
+    if (!finite3(R) || smin3(R.x, R.y, R.z) < 0) {
+        raise(E, P, st.pixel[path], st.sample[path], kErrNonFiniteRadiance);
+        R = V3{};
+    }
+    st.out[path] = f4(R, 0);
+}
+
+// One iteration of trace()'s bounce loop (render.cpp:240-344) for one path, after its
+// closest hit is known. Sets cont when the path continues, shadow when a shadow ray was
+// queued; a path that ends with a queued shadow ray is finished by k_shadow.
+CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
+                   unsigned long long* retries, bool& cont, bool& shadow) {
+    cont = false; shadow = false;
+    uint32_t flags = st.flags[path];
+    const bool precise = flags & kPathPrecise;
+    const TRay ray = loadRay(st, path, flags);
+    const float4 th = st.thr[path], ra = st.rad[path], ab = st.absorb[path];
+    V3 T = v3(th), R = v3(ra), A = v3(ab);
+    float etaScale = th.w, lastPdf = ra.w;
+    int medium = __float_as_int(ab.w);
+    bool lastDelta = flags & kPathLastDelta;
+    const V3 lastPosition = v3(st.last_pos[path]);
+    const uint32_t depth = st.depth[path];
+    const uint32_t pixel = st.pixel[path], sample = st.sample[path];
+    Rng rng(st.rng[path]);
+    const uint32_t tri = st.hit_tri[path];
+    int err = 0;
+
+    if (tri == kNoTriangle) {  // render.cpp:242-248
+        if (medium >= 0) T = T * beerLambert(A, kInf);
+        const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, environmentPdf(S, ray.d));
+        R = R + T * envRadiance(S, ray.d) * weight;
+        finishPath(P, st, path, R, E);
+        return;
+    }
+    // The traversal reported the triangle; t, u and v come from the same FP64 arithmetic.
+    const cr_triangle& tr = S.tris[tri];
+    const ExactSetup X = exact_setup(ray);
+    double t = 0, w1 = 0, w2 = 0, det = 1;
+    tri_exact(X, v3(tr.v[0].position), v3(tr.v[1].position), v3(tr.v[2].position), -static_cast<double>(kInf),
+              static_cast<double>(kInf), t, w1, w2, det);
+    const double hu = w1 / det, hv = w2 / det;
+    if (medium >= 0) T = T * beerLambert(A, static_cast<float>(t));
+    const Surface s = surfaceAt(S, ray.d, tri, hu, hv, err);
+    if (s.frontFace || s.doubleSided) {
+        const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, trianglePdf(S, tri, lastPosition, s.position));
+        R = R + T * s.emission * weight;
+    }
+    if (static_cast<int>(depth) == P.bounces) {
+        if (err) { raise(E, P, pixel, sample, err); }
+        finishPath(P, st, path, R, E);
+        return;
+    }
+    const V3 wo = -ray.d;
+    bool pending = false;
+    TRay sh;
+    V3 contrib;
+    if (P.nee) {  // render.cpp:262-299
+        const LightSample light = sampleLight(S, s.position, rng, P.env_alias, err);
+        const bool enclosedInfinite = medium >= 0 && s.thickness <= 0 && !isfin(light.distance);
+        if (!enclosedInfinite && light.pdf > 0 && maxComponent(light.radiance) > 0) {
+            const BsdfEval bsdf = evaluateBsdf(s, wo, light.direction);
+            if (maxComponent(bsdf.value) > 0) {
+                bool ok = true;
+                if (precise) { sh.o = s.position; sh.d = light.direction; sh.tmin = 0; sh.tmax = kInf; sh.olow = s.positionLow; }
+                else ok = offsetRay(s.position, s.geometricNormal, light.direction, kInf, sh, err);
+                if (ok && isfin(light.distance)) {
+                    V3 end = light.target;
+                    if (lengthSquared(light.targetNormal) > 0) {
+                        TRay moved;
+                        ok = offsetRay(end, light.targetNormal, -light.direction, kInf, moved, err);
+                        end = moved.o;
+                    }
+                    const V3 delta = end - sh.o;
+                    sh.tmax = length(delta) * (1 - 2e-6f);
+                    sh.d = normalize(delta);
+                }
+                if (ok) {
+                    const float weight = light.delta ? 1 : powerHeuristic(light.pdf, bsdf.pdf);
+                    V3 shadowAbsorption = A;
+                    bool shadowInMedium = medium >= 0;
+                    if (s.thickness > 0 && dot(wo, s.geometricNormal) * dot(light.direction, s.geometricNormal) < 0) {
+                        shadowInMedium = s.frontFace;
+                        shadowAbsorption = s.frontFace ? absorptionCoefficient(s.attenuationColor, s.attenuationDistance) : V3{};
+                    }
+                    const V3 transmittance = shadowInMedium ? beerLambert(shadowAbsorption, light.distance) : V3{1};
+                    contrib = T * bsdf.value * light.radiance * transmittance *
+                              (fabsf(dot(s.normal, light.direction)) * weight / light.pdf);
+                    pending = true;
+                }
+            }
+        }
+    }
+    if (err) {  // an exception inside trace(): the sample fails
+        raise(E, P, pixel, sample, err);
+        finishPath(P, st, path, V3{}, E);
+        return;
+    }
+    const uint32_t ignore = precise ? tri : kNoTriangle;
+    auto queueShadow = [&](bool dead) {
+        st.sh_o[path] = f4(sh.o, sh.tmin);
+        st.sh_d[path] = f4(sh.d, sh.tmax);
+        st.sh_lo[path] = f4(sh.olow, __uint_as_float(ignore));
+        st.sh_c[path] = f4(contrib, 0);
+        shadow = true;
+        if (dead) {
+            st.rad[path] = f4(R, lastPdf);
+            st.flags[path] = flags | kPathDead | kPathShadow;
+        }
+    };
+    const BsdfSample smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
+    if (!smp.ok()) {
+        if (pending) queueShadow(true); else finishPath(P, st, path, R, E);
+        return;
+    }
+    T = T * smp.weight;
+    if (!finite3(T)) {
+        raise(E, P, pixel, sample, kErrNonFiniteThroughput);
+        finishPath(P, st, path, V3{}, E);
+        return;
+    }
+    int boundary = 0;
+    if (smp.transmitted && s.thickness > 0) {  // render.cpp:306-329
+        if (s.frontFace) {
+            if (medium >= 0) boundary = kErrNestedVolume;
+            else { medium = static_cast<int>(s.material); A = absorptionCoefficient(s.attenuationColor, s.attenuationDistance); }
+        } else {
+            if (medium < 0) boundary = kErrExitWithoutEntry;
+            else { medium = -1; A = V3{}; }
+        }
+        if (!boundary) etaScale *= smp.eta * smp.eta;
+    }
+    if (boundary) {
+        if (!precise) {  // render.cpp:404-411: replay the same sample from split origins
+            atomicAdd(retries, 1ull);
+            initPath(S, P, st, path, pixel, sample, true, E);
+            cont = true;
+            return;
+        }
+        raise(E, P, pixel, sample, boundary);
+        if (E.detail && boundary == kErrExitWithoutEntry) {
+            E.detail->depth = static_cast<int32_t>(depth);
+            E.detail->triangle = tri;
+            E.detail->material = s.material;
+            E.detail->t = t;
+            E.detail->point[0] = s.position.x; E.detail->point[1] = s.position.y; E.detail->point[2] = s.position.z;
+            E.detail->origin[0] = ray.o.x; E.detail->origin[1] = ray.o.y; E.detail->origin[2] = ray.o.z;
+            E.detail->direction[0] = ray.d.x; E.detail->direction[1] = ray.d.y; E.detail->direction[2] = ray.d.z;
+        }
+        finishPath(P, st, path, V3{}, E);
+        return;
+    }
+    lastPdf = smp.pdf;
+    lastDelta = smp.delta;
+    TRay next;
+    if (precise) { next.o = s.position; next.d = smp.direction; next.tmin = 0; next.tmax = kInf; next.olow = s.positionLow; }
+    else if (!offsetRay(s.position, s.geometricNormal, smp.direction, kInf, next, err)) {
+        raise(E, P, pixel, sample, err);
+        finishPath(P, st, path, V3{}, E);
+        return;
+    }
+    if (P.rr && depth >= 3) {  // render.cpp:337-343
+        const float survive = sclamp(maxComponent(T) * etaScale, 0.05f, 0.95f);
+        if (rng.uniform() >= survive) {
+            if (pending) queueShadow(true); else finishPath(P, st, path, R, E);
+            return;
+        }
+        T = T * (1 / survive);
+    }
+    // continue
+    st.ray_o[path] = f4(next.o, next.tmin);
+    st.ray_d[path] = f4(next.d, next.tmax);
+    if (precise) st.ray_lo[path] = f4(next.olow, 0);
+    st.thr[path] = f4(T, etaScale);
+    st.rad[path] = f4(R, lastPdf);
+    st.last_pos[path] = f4(s.position, 0);
+    st.absorb[path] = f4(A, __int_as_float(medium));
+    flags = (flags & kPathPrecise) | (lastDelta ? kPathLastDelta : 0u);
+    st.flags[path] = flags;
+    st.rng[path] = rng.state;
+    st.prev_tri[path] = ignore;
+    st.depth[path] = depth + 1;
+    if (pending) queueShadow(false);
+    cont = true;
+}
+
+// ---- kernels ---------------------------------------------------------------------------------
+__global__ void k_generate(DevScene S, RenderParams P, PathSoA st, Queues q, WaveInfo w, ErrSink E) {
+    for (uint32_t base = blockIdx.x * blockDim.x; base < w.paths; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        bool live = false;
+        if (i < w.paths) {
+            const uint32_t pixel = w.pixel0 + i % w.npix, sample = w.sample0 + i / w.npix;
+            live = initPath(S, P, st, i, pixel, sample, false, E);
+            if (!live) st.out[i] = make_float4(0, 0, 0, 0);
+        }
+        warpPush(q.extend[0], &q.counts[kCountExtend0], live, i);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_extend(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, ErrSink E,
+                                                unsigned long long* stats) {
+    const uint32_t n = q.counts[cur];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        q.counts[cur ^ 1] = 0;
+        q.counts[kCountShadow] = 0;
+        stats[kStatExtendRays] += n;
+    }
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const uint32_t path = q.extend[cur][idx];
+        const uint32_t flags = st.flags[path];
+        const TRay r = loadRay(st, path, flags);
+        HitRec h;
+        h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
+        int err = 0;
+        const bool found = intersect<false>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0, h, err);
+        st.hit_tri[path] = found ? h.tri : kNoTriangle;
+        if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, ErrSink E,
+                                               unsigned long long* stats) {
+    const uint32_t n = q.counts[cur];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        bool cont = false, shadow = false;
+        uint32_t path = 0;
+        if (idx < n) {
+            path = q.extend[cur][idx];
+            shadeOne(S, P, st, path, E, &stats[kStatRetries], cont, shadow);
+        }
+        warpPush(q.extend[cur ^ 1], &q.counts[cur ^ 1], cont, path);
+        warpPush(q.shadow, &q.counts[kCountShadow], shadow, path);
+    }
+}
+
+CR_D void shadowOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E) {
+    const float4 o = st.sh_o[path], d = st.sh_d[path], lo = st.sh_lo[path], c = st.sh_c[path];
+    TRay r;
+    r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w; r.olow = v3(lo);
+    HitRec h;
+    h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
+    int err = 0;
+    const bool blocked = intersect<true>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0, h, err);
+    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    const float4 ra = st.rad[path];
+    V3 R = v3(ra);
+    if (!blocked) R = R + v3(c);
+    const uint32_t flags = st.flags[path];
+    if (flags & kPathDead) finishPath(P, st, path, R, E);
+    else st.rad[path] = f4(R, ra.w);
+}
+
+__global__ void __launch_bounds__(128) k_shadow(DevScene S, RenderParams P, PathSoA st, Queues q, ErrSink E,
+                                                unsigned long long* stats) {
+    const uint32_t n = q.counts[kCountShadow];
+    if (blockIdx.x == 0 && threadIdx.x == 0) stats[kStatShadowRays] += n;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x)
+        shadowOne(S, P, st, q.shadow[idx], E);
+}
+
+// render.cpp:390-413: each pixel adds its samples in index order.
+__global__ void k_accumulate(PathSoA st, WaveInfo w, double* acc) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.npix; i += gridDim.x * blockDim.x) {
+        const uint64_t p = static_cast<uint64_t>(w.pixel0) + i;
+        double r = acc[3 * p], g = acc[3 * p + 1], b = acc[3 * p + 2];
+        for (uint32_t k = 0; k < w.nsamp; ++k) {
+            const float4 o = st.out[static_cast<uint64_t>(k) * w.npix + i];
+            r += o.x; g += o.y; b += o.z;
+        }
+        acc[3 * p] = r; acc[3 * p + 1] = g; acc[3 * p + 2] = b;
+    }
+}
+// Optional copy of every sample's radiance (sample-major) for stream-level comparisons.
+__global__ void k_dump_samples(PathSoA st, WaveInfo w, uint64_t pixels, float* dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.paths; i += gridDim.x * blockDim.x) {
+        const uint64_t p = w.pixel0 + i % w.npix, s = w.sample0 + i / w.npix;
+        const float4 o = st.out[i];
+        float* d = dst + 3 * (s * pixels + p);
+        d[0] = o.x; d[1] = o.y; d[2] = o.z;
+    }
+}
+// render.cpp:415
+__global__ void k_film(const double* acc, float* film, uint64_t pixels, int samples) {
+    for (uint64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * pixels; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        film[i] = static_cast<float>(acc[i] / samples);
+}
+
+// Re-runs one failing sample on one thread with full error capture (same device functions).
+__global__ void k_trace_one(DevScene S, RenderParams P, PathSoA st, uint32_t pixel, uint32_t sample, DevError* detail,
+                            unsigned long long* scratchKey, unsigned long long* scratchRetries) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const ErrSink E{scratchKey, detail};
+    const uint32_t path = 0;
+    if (!initPath(S, P, st, path, pixel, sample, false, E)) return;
+    for (int iter = 0; iter < 4 * (P.bounces + 2); ++iter) {
+        const uint32_t flags = st.flags[path];
+        const TRay r = loadRay(st, path, flags);
+        HitRec h;
+        h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
+        int err = 0;
+        const bool found = intersect<false>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0, h, err);
+        if (err) { raise(E, P, pixel, sample, err); return; }
+        st.hit_tri[path] = found ? h.tri : kNoTriangle;
+        bool cont = false, shadow = false;
+        shadeOne(S, P, st, path, E, scratchRetries, cont, shadow);
+        if (detail->code) return;
+        if (shadow) shadowOne(S, P, st, path, E);
+        if (detail->code || !cont) return;
+    }
+}
+
+__global__ void k_intersect_batch(DevScene S, const cr_ray* rays, cr_hit* hits, uint8_t* found, uint64_t n, int any,
+                                  uint32_t ignore, int exact, unsigned long long* errIndex) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const cr_ray cr = rays[i];
+        TRay r;
+        r.o = v3(cr.origin); r.d = v3(cr.direction); r.tmin = cr.tmin; r.tmax = cr.tmax; r.olow = v3(cr.origin_low);
+        const cr_hit in = hits[i];
+        HitRec h{in.t, in.u, in.v, in.triangle};
+        int err = 0;
+        const bool f = any ? intersect<true>(S, r, in.t, ignore, exact != 0, h, err)
+                           : intersect<false>(S, r, in.t, ignore, exact != 0, h, err);
+        if (f) { cr_hit out = in; out.t = h.t; out.u = h.u; out.v = h.v; out.triangle = h.tri; hits[i] = out; }
+        found[i] = f ? 1 : 0;
+        if (err) atomicMin(errIndex, static_cast<unsigned long long>(i));
+    }
+}
+
+__global__ void k_camera_rays(RenderParams P, uint32_t sample, cr_ray* out, unsigned long long* errKey) {
+    const uint64_t pixels = static_cast<uint64_t>(P.width) * P.height;
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < pixels; p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        Rng rng(sampleSeed(P.seed, p, sample));
+        const uint32_t x = static_cast<uint32_t>(p % P.width), y = static_cast<uint32_t>(p / P.width);
+        const float dx = rng.uniform(), dy = rng.uniform();
+        TRay r;
+        cr_ray o;
+        if (!cameraRay(P.camera, P.width, P.height, static_cast<float>(x) + dx, static_cast<float>(y) + dy, r)) {
+            atomicMin(errKey, static_cast<unsigned long long>(errorKey(P, static_cast<uint32_t>(p), sample)));
+            memset(&o, 0, sizeof(o));
+        } else {
+            o.origin[0] = r.o.x; o.origin[1] = r.o.y; o.origin[2] = r.o.z;
+            o.direction[0] = r.d.x; o.direction[1] = r.d.y; o.direction[2] = r.d.z;
+            o.tmin = r.tmin; o.tmax = r.tmax;
+            o.origin_low[0] = o.origin_low[1] = o.origin_low[2] = 0;
+        }
+        out[p] = o;
+    }
+}
+
+}  // namespace crg
+
+// =============================================================================================
+// Host driver
+// =============================================================================================
+using namespace crg;
+
+namespace {
+
+struct CudaError : crh::Error {
+    CudaError(cudaError_t e, const char* what)
+        : crh::Error(e == cudaErrorMemoryAllocation ? CR_ERR_OUT_OF_MEMORY : CR_ERR_CUDA,
+                     std::string(what) + ": " + cudaGetErrorString(e)) {}
+};
+#define CR_CUDA(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) throw CudaError(e_, #call); } while (0)
+
+// Device allocation owned by a scene.
+struct DevAlloc {
+    std::vector<void*> blocks;
+    uint64_t bytes = 0;
+    template <class T> T* alloc(size_t count) {
+        if (count == 0) count = 1;
+        void* p = nullptr;
+        CR_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        blocks.push_back(p);
+        bytes += count * sizeof(T);
+        return static_cast<T*>(p);
+    }
+    template <class T> T* upload(const T* src, size_t count, cudaStream_t s) {
+        T* d = alloc<T>(count);
+        if (count) CR_CUDA(cudaMemcpyAsync(d, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+        return d;
+    }
+    void release() {
+        for (void* p : blocks) cudaFree(p);
+        blocks.clear();
+        bytes = 0;
+    }
+};
+
+int occupancyGrid(const void* kernel, int block, int device) {
+    int sms = 0, perSm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, block, 0);
+    if (perSm < 1) perSm = 1;
+    return sms * perSm;
+}
+
+}  // namespace
+
+struct cr_gpu_scene {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevAlloc geometry;  // scene data
+    DevAlloc work;      // path buffers
+    DevScene dev{};
+    uint64_t triangleCount = 0;
+    // work buffers
+    size_t capacity = 0;
+    PathSoA st{};
+    Queues q{};
+    uint32_t* counts = nullptr;
+    unsigned long long* stats = nullptr;
+    DevError* detail = nullptr;
+    double* acc = nullptr;
+    float* film = nullptr;
+    size_t filmPixels = 0;
+    DevAlloc filmAlloc;
+    uint32_t* hostCounts = nullptr;           // pinned
+    unsigned long long* hostStats = nullptr;  // pinned
+    int gridExtend = 0, gridShade = 0, gridShadow = 0, gridSmall = 0;
+    std::vector<cudaEvent_t> events;
+    cr_render_options lastOptions{};
+    std::mutex mutex;
+
+    ~cr_gpu_scene() {
+        if (device >= 0) cudaSetDevice(device);
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        if (stream) cudaStreamSynchronize(stream);
+        geometry.release();
+        work.release();
+        filmAlloc.release();
+        if (hostCounts) cudaFreeHost(hostCounts);
+        if (hostStats) cudaFreeHost(hostStats);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    cudaEvent_t event(size_t i) {
+        while (events.size() <= i) {
+            cudaEvent_t e;
+            CR_CUDA(cudaEventCreate(&e));
+            events.push_back(e);
+        }
+        return events[i];
+    }
+
+    void ensureWork(size_t paths) {
+        if (paths <= capacity) return;
+        CR_CUDA(cudaStreamSynchronize(stream));
+        work.release();
+        const size_t n = paths;
+        st.ray_o = work.alloc<float4>(n); st.ray_d = work.alloc<float4>(n); st.ray_lo = work.alloc<float4>(n);
+        st.hit_tri = work.alloc<uint32_t>(n);
+        st.thr = work.alloc<float4>(n); st.rad = work.alloc<float4>(n); st.last_pos = work.alloc<float4>(n);
+        st.absorb = work.alloc<float4>(n); st.flags = work.alloc<uint32_t>(n);
+        st.rng = work.alloc<uint64_t>(n); st.prev_tri = work.alloc<uint32_t>(n);
+        st.pixel = work.alloc<uint32_t>(n); st.sample = work.alloc<uint32_t>(n); st.depth = work.alloc<uint32_t>(n);
+        st.sh_o = work.alloc<float4>(n); st.sh_d = work.alloc<float4>(n); st.sh_lo = work.alloc<float4>(n);
+        st.sh_c = work.alloc<float4>(n); st.out = work.alloc<float4>(n);
+        q.extend[0] = work.alloc<uint32_t>(n); q.extend[1] = work.alloc<uint32_t>(n); q.shadow = work.alloc<uint32_t>(n);
+        counts = work.alloc<uint32_t>(kCountWords);
+        q.counts = counts;
+        stats = work.alloc<unsigned long long>(kStatWords);
+        detail = work.alloc<DevError>(1);
+        capacity = n;
+    }
+
+    void ensureFilm(size_t pixels) {
+        if (pixels <= filmPixels) return;
+        CR_CUDA(cudaStreamSynchronize(stream));
+        filmAlloc.release();
+        acc = filmAlloc.alloc<double>(3 * pixels);
+        film = filmAlloc.alloc<float>(3 * pixels);
+        filmPixels = pixels;
+    }
+};
+
+namespace {
+
+cr_status fail(const std::exception& e) {
+    if (const auto* x = dynamic_cast<const crh::Error*>(&e)) return crh::set_last_error(x->status, x->what());
+    if (dynamic_cast<const std::bad_alloc*>(&e)) return crh::set_last_error(CR_ERR_OUT_OF_MEMORY, "host allocation failed");
+    return crh::set_last_error(CR_ERR_CUDA, e.what());
+}
+
+// Build the device scene: geometry in leaf order, node pairs, materials, lights, environment.
+void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_desc& env) {
+    const uint64_t n = d.triangle_count;
+    if (n && !d.triangles) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "triangles is NULL");
+    if (d.material_count && !d.materials) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "materials is NULL");
+    for (uint64_t i = 0; i < n; ++i)
+        if (d.triangles[i].material >= d.material_count) throw crh::Error(CR_ERR_OUT_OF_RANGE, "Triangle material index out of range");
+    for (uint32_t m = 0; m < d.material_count; ++m) {
+        const cr_material& mat = d.materials[m];
+        const cr_texture_slot* s[5] = {&mat.base_color_texture, &mat.metallic_roughness_texture, &mat.normal_texture,
+                                       &mat.emissive_texture, &mat.transmission_texture};
+        for (auto* slot : s) {
+            if (slot->texture == -1) continue;
+            if (slot->texture < 0 || static_cast<uint32_t>(slot->texture) >= d.texture_count)
+                throw crh::Error(CR_ERR_OUT_OF_RANGE, "Texture slot index out of range");
+            if (slot->texcoord < 0 || slot->texcoord > 1) throw crh::Error(CR_ERR_OUT_OF_RANGE, "Only TEXCOORD_0 and TEXCOORD_1 are supported");
+            const cr_texture& t = d.textures[slot->texture];
+            if (t.image < 0 || static_cast<uint32_t>(t.image) >= d.image_count) throw crh::Error(CR_ERR_OUT_OF_RANGE, "Texture image index out of range");
+            const cr_image& im = d.images[t.image];
+            if (im.width <= 0 || im.height <= 0 || !im.pixels) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "Texture image dimensions do not match its pixels");
+        }
+    }
+    // BVH: the caller's (the reference's own node array) or ours.
+    std::vector<cr_bvh_node> nodes;
+    std::vector<uint32_t> indices;
+    if (d.bvh_nodes && d.bvh_node_count) {
+        nodes.assign(d.bvh_nodes, d.bvh_nodes + d.bvh_node_count);
+        indices.assign(d.bvh_indices, d.bvh_indices + d.bvh_index_count);
+    } else {
+        crh::build_bvh(d.triangles, n, nodes, indices);
+    }
+    // Structure checks: adjacent children at odd indices, leaf ranges inside indices.
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        const cr_bvh_node& nd = nodes[i];
+        if (nd.count) {
+            if (static_cast<uint64_t>(nd.first) + nd.count > indices.size()) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH leaf range outside its index array");
+        } else if ((nd.first & 1u) == 0 || static_cast<uint64_t>(nd.first) + 1 >= nodes.size() || nd.first <= i) {
+            throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH interior node does not reference an adjacent child pair");
+        }
+    }
+    for (uint32_t idx : indices) if (idx >= n) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH index outside the triangle array");
+
+    cudaStream_t s = g.stream;
+    DevScene& S = g.dev;
+    S = DevScene{};
+    S.triangle_count = n;
+    g.triangleCount = n;
+    // per-triangle flags and geometric normals (Scene::accepts, geometry.cpp:282-290)
+    std::vector<float4> ng(n ? n : 1);
+    std::vector<uint32_t> flags(n ? n : 1, 0);
+    uint32_t anyMask = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const cr_triangle& t = d.triangles[i];
+        const cr_material& m = d.materials[t.material];
+        uint32_t f = 0;
+        if (!m.double_sided && m.transmission <= 0) f |= kTriCull;
+        if (m.alpha_mode == CR_ALPHA_MASK) { f |= kTriAlphaMask; anyMask = 1; }
+        flags[i] = f;
+        float gx = t.geometric_normal[0], gy = t.geometric_normal[1], gz = t.geometric_normal[2];
+        if (gx == 0 && gy == 0 && gz == 0) {  // geometry.cpp:284
+            const double ax = static_cast<double>(t.v[1].position[0]) - t.v[0].position[0];
+            const double ay = static_cast<double>(t.v[1].position[1]) - t.v[0].position[1];
+            const double az = static_cast<double>(t.v[1].position[2]) - t.v[0].position[2];
+            const double bx = static_cast<double>(t.v[2].position[0]) - t.v[0].position[0];
+            const double by = static_cast<double>(t.v[2].position[1]) - t.v[0].position[1];
+            const double bz = static_cast<double>(t.v[2].position[2]) - t.v[0].position[2];
+            const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+            const double sq = cx * cx + cy * cy + cz * cz;
+            if (sq > 0 && std::isfinite(sq)) {
+                const double inv = 1 / std::sqrt(sq);
+                gx = static_cast<float>(cx * inv); gy = static_cast<float>(cy * inv); gz = static_cast<float>(cz * inv);
+            }
+        }
+        uint32_t fb = f;
+        float fw;
+        std::memcpy(&fw, &fb, 4);
+        ng[i] = make_float4(gx, gy, gz, fw);
+    }
+    std::vector<float4> pos(3 * (indices.empty() ? 1 : indices.size()));
+    for (size_t slot = 0; slot < indices.size(); ++slot) {
+        const uint32_t idx = indices[slot];
+        const cr_triangle& t = d.triangles[idx];
+        float w0, w1;
+        std::memcpy(&w0, &idx, 4);
+        std::memcpy(&w1, &flags[idx], 4);
+        pos[3 * slot] = make_float4(t.v[0].position[0], t.v[0].position[1], t.v[0].position[2], w0);
+        pos[3 * slot + 1] = make_float4(t.v[1].position[0], t.v[1].position[1], t.v[1].position[2], w1);
+        pos[3 * slot + 2] = make_float4(t.v[2].position[0], t.v[2].position[1], t.v[2].position[2], 0.0f);
+    }
+    const size_t pairCount = nodes.size() > 1 ? (nodes.size() - 1) / 2 : 0;
+    std::vector<NodePair> pairs(pairCount ? pairCount : 1);
+    auto childRef = [&](const cr_bvh_node& c, uint32_t& ref, uint32_t& cnt) {
+        if (c.count) { ref = c.first; cnt = c.count; } else { ref = (c.first - 1) / 2; cnt = 0; }
+    };
+    for (size_t p = 0; p < pairCount; ++p) {
+        const cr_bvh_node& c0 = nodes[2 * p + 1];
+        const cr_bvh_node& c1 = nodes[2 * p + 2];
+        NodePair& np = pairs[p];
+        np.a = make_float4(c0.lo[0], c0.lo[1], c0.lo[2], c0.hi[0]);
+        np.b = make_float4(c0.hi[1], c0.hi[2], c1.lo[0], c1.lo[1]);
+        np.c = make_float4(c1.lo[2], c1.hi[0], c1.hi[1], c1.hi[2]);
+        childRef(c0, np.d.x, np.d.y);
+        childRef(c1, np.d.z, np.d.w);
+    }
+    if (!nodes.empty()) {
+        S.has_root = 1;
+        for (int k = 0; k < 3; ++k) { S.root_lo[k] = nodes[0].lo[k]; S.root_hi[k] = nodes[0].hi[k]; }
+        childRef(nodes[0], S.root_ref, S.root_count);
+    }
+    S.tri_pos = g.geometry.upload(pos.data(), pos.size(), s);
+    S.tri_ng = g.geometry.upload(ng.data(), ng.size(), s);
+    S.tris = g.geometry.upload(d.triangles, n ? n : 0, s);
+    S.pairs = g.geometry.upload(pairs.data(), pairs.size(), s);
+    S.any_alpha_mask = anyMask;
+    // materials and textures
+    S.materials = g.geometry.upload(d.materials, d.material_count, s);
+    S.material_count = d.material_count;
+    std::vector<double2> trig(5 * (d.material_count ? d.material_count : 1));
+    for (uint32_t m = 0; m < d.material_count; ++m) {
+        const cr_material& mat = d.materials[m];
+        const cr_texture_slot* sl[5] = {&mat.base_color_texture, &mat.metallic_roughness_texture, &mat.normal_texture,
+                                        &mat.emissive_texture, &mat.transmission_texture};
+        for (int k = 0; k < 5; ++k) {
+            const double r = static_cast<double>(sl[k]->rotation);
+            trig[5 * m + k] = make_double2(std::cos(r), std::sin(r));
+        }
+    }
+    S.slot_trig = g.geometry.upload(trig.data(), trig.size(), s);
+    std::vector<DevImage> images(d.image_count ? d.image_count : 1);
+    for (uint32_t i = 0; i < d.image_count; ++i) {
+        images[i].width = d.images[i].width; images[i].height = d.images[i].height;
+        const size_t px = static_cast<size_t>(d.images[i].width) * d.images[i].height;
+        images[i].pixels = g.geometry.upload(reinterpret_cast<const float4*>(d.images[i].pixels), px, s);
+    }
+    S.images = g.geometry.upload(images.data(), images.size(), s);
+    S.image_count = d.image_count;
+    S.textures = g.geometry.upload(d.textures, d.texture_count, s);
+    S.texture_count = d.texture_count;
+    // environment
+    crh::EnvTables E;
+    crh::build_environment(env, E);
+    S.env_has_image = E.hasImage;
+    for (int k = 0; k < 3; ++k) S.env_constant[k] = E.constant[k];
+    if (E.hasImage) {
+        S.env_width = E.width; S.env_height = E.height;
+        const size_t px = static_cast<size_t>(E.width) * E.height;
+        S.env_pixels = g.geometry.upload(reinterpret_cast<const float4*>(env.pixels), px, s);
+        S.env_cdf = g.geometry.upload(E.cdf.data(), E.cdf.size(), s);
+        S.env_pdf = g.geometry.upload(E.pdf.data(), E.pdf.size(), s);
+        S.env_row_cos = g.geometry.upload(E.rowCos.data(), E.rowCos.size(), s);
+        S.env_coarse = g.geometry.upload(E.coarse.data(), E.coarse.size(), s);
+        S.env_coarse_count = static_cast<uint32_t>(E.coarse.size());
+        S.alias_prob = g.geometry.upload(E.aliasProb.data(), E.aliasProb.size(), s);
+        S.alias_index = g.geometry.upload(E.aliasIndex.data(), E.aliasIndex.size(), s);
+    }
+    S.env_weight_sum = E.weightSum;
+    S.env_rotation = E.rotation;
+    S.env_intensity = E.intensity;
+    // lights
+    crh::LightTables L;
+    crh::build_lights(d.triangles, n, d.materials, d.lights, d.light_count, E.integral, L);
+    S.light_entries = g.geometry.upload(L.entries.data(), L.entries.size(), s);
+    S.light_entry_count = static_cast<uint32_t>(L.entries.size());
+    S.tri_light_probability = g.geometry.upload(L.triangleProbability.data(), L.triangleProbability.size(), s);
+    S.env_probability = L.environmentProbability;
+    std::vector<DevPunctual> punctual(d.light_count ? d.light_count : 1);
+    for (uint32_t i = 0; i < d.light_count; ++i) {
+        const cr_punctual_light& l = d.lights[i];
+        DevPunctual& p = punctual[i];
+        p.type = l.type;
+        for (int k = 0; k < 3; ++k) { p.position[k] = l.position[k]; p.direction[k] = l.direction[k]; p.color[k] = l.color[k]; }
+        p.intensity = l.intensity; p.range = l.range;
+        p.cos_outer = std::cos(l.outer_cone);  // render.cpp:203 (float std::cos)
+        p.cos_inner = std::cos(l.inner_cone);
+    }
+    S.punctual = g.geometry.upload(punctual.data(), punctual.size(), s);
+    S.punctual_count = d.light_count;
+    CR_CUDA(cudaStreamSynchronize(s));
+}
+
+RenderParams makeParams(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, const cr_gpu_tuning& t) {
+    RenderParams P{};
+    P.width = o.width; P.height = o.height; P.samples = o.samples; P.bounces = o.bounces;
+    P.seed = o.seed; P.nee = o.next_event_estimation != 0; P.rr = o.russian_roulette != 0;
+    P.env_alias = t.env_alias; P.exact_traversal = t.exact_traversal;
+    crh::camera_setup(camera, o.width, o.height, P.camera);
+    (void)g;
+    return P;
+}
+
+int referenceWorkers(const cr_render_options& o) {  // render.cpp:361-363
+    constexpr int tileSize = 16;
+    const int tilesX = (o.width + tileSize - 1) / tileSize, tilesY = (o.height + tileSize - 1) / tileSize, tiles = tilesX * tilesY;
+    const int automatic = static_cast<int>(std::max(1u, std::thread::hardware_concurrency() / 2));
+    return std::min(tiles, o.threads ? o.threads : automatic);
+}
+
+// The whole render. film_host may be NULL (film stays on the device).
+void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, cr_progress_fn progress,
+                void* user, float* filmHost, cr_render_stats* stats, const cr_gpu_tuning& tuning, float* perSample) {
+    const auto start = std::chrono::steady_clock::now();
+    crh::validate_options(o);
+    const uint64_t pixels = static_cast<uint64_t>(o.width) * o.height;
+    const uint64_t total = pixels * static_cast<uint64_t>(o.samples);
+    RenderParams P;
+    try {
+        P = makeParams(g, camera, o, tuning);
+    } catch (const crh::Error& e) {
+        // The reference throws these from Camera::generate inside the first sample.
+        throw crh::Error(CR_ERR_RENDER, std::string("Pixel (0,0), sample 0: ") + e.what());
+    }
+    CR_CUDA(cudaSetDevice(g.device));
+    // Wave plan: up to `target` path slots; whole pixel range with several samples, or pixel
+    // chunks with one sample.
+    uint64_t target = tuning.paths_per_wave > 0 ? static_cast<uint64_t>(tuning.paths_per_wave) : (uint64_t{1} << 21);
+    if (target < 1024) target = 1024;
+    uint32_t npix, nsamp;
+    if (pixels <= target) {
+        npix = static_cast<uint32_t>(pixels);
+        nsamp = static_cast<uint32_t>(std::min<uint64_t>(o.samples, std::max<uint64_t>(1, target / pixels)));
+    } else {
+        npix = static_cast<uint32_t>(target);
+        nsamp = 1;
+    }
+    g.ensureWork(static_cast<size_t>(npix) * nsamp);
+    g.ensureFilm(pixels);
+    if (!g.hostCounts) CR_CUDA(cudaMallocHost(&g.hostCounts, kCountWords * sizeof(uint32_t)));
+    if (!g.hostStats) CR_CUDA(cudaMallocHost(&g.hostStats, kStatWords * sizeof(unsigned long long)));
+    cudaStream_t s = g.stream;
+    const int block = tuning.block_size > 0 ? tuning.block_size : 128;
+    if (!g.gridExtend) {
+        g.gridExtend = occupancyGrid(reinterpret_cast<const void*>(k_extend), 128, g.device);
+        g.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade), 128, g.device);
+        g.gridShadow = occupancyGrid(reinterpret_cast<const void*>(k_shadow), 128, g.device);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
+        g.gridSmall = sms * 8;
+    }
+    (void)block;
+    CR_CUDA(cudaMemsetAsync(g.acc, 0, 3 * pixels * sizeof(double), s));
+    CR_CUDA(cudaMemsetAsync(g.stats, 0, kStatWords * sizeof(unsigned long long), s));
+    const unsigned long long noError = ~0ull;
+    CR_CUDA(cudaMemcpyAsync(g.stats + kStatErrorKey, &noError, sizeof(noError), cudaMemcpyHostToDevice, s));
+    const ErrSink E{g.stats + kStatErrorKey, nullptr};
+
+    const bool timePhases = tuning.time_phases != 0;
+    double extendMs = 0, shadeMs = 0, shadowMs = 0;
+    uint64_t launches = 0;
+    int waves = 0;
+    cudaEvent_t t0 = g.event(0), t1 = g.event(1);
+    CR_CUDA(cudaEventRecord(t0, s));
+    auto lastProgress = start;
+    uint64_t done = 0;
+    bool errored = false;
+    for (uint32_t s0 = 0; s0 < static_cast<uint32_t>(o.samples) && !errored; s0 += nsamp) {
+        const uint32_t ns = std::min<uint32_t>(nsamp, static_cast<uint32_t>(o.samples) - s0);
+        for (uint64_t p0 = 0; p0 < pixels && !errored; p0 += npix) {
+            WaveInfo w;
+            w.pixel0 = static_cast<uint32_t>(p0);
+            w.npix = static_cast<uint32_t>(std::min<uint64_t>(npix, pixels - p0));
+            w.sample0 = s0; w.nsamp = ns; w.paths = w.npix * ns;
+            ++waves;
+            CR_CUDA(cudaMemsetAsync(g.counts, 0, kCountWords * sizeof(uint32_t), s));
+            k_generate<<<g.gridSmall, 128, 0, s>>>(g.dev, P, g.st, g.q, w, E);
+            ++launches;
+            int cur = 0;
+            size_t ev = 2;
+            std::vector<std::pair<size_t, int>> timed;  // (event index, phase)
+            auto bounce = [&]() {
+                auto rec = [&](int phase, auto&& launch) {
+                    if (timePhases) { CR_CUDA(cudaEventRecord(g.event(ev), s)); }
+                    launch();
+                    if (timePhases) { CR_CUDA(cudaEventRecord(g.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
+                    ++launches;
+                };
+                rec(0, [&] { k_extend<<<g.gridExtend, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats); });
+                rec(1, [&] { k_shade<<<g.gridShade, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats); });
+                rec(2, [&] { k_shadow<<<g.gridShadow, 128, 0, s>>>(g.dev, P, g.st, g.q, E, g.stats); });
+                cur ^= 1;
+            };
+            for (int b = 0; b <= o.bounces; ++b) bounce();
+            CR_CUDA(cudaMemcpyAsync(g.hostCounts, g.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaStreamSynchronize(s));
+            if (g.hostCounts[cur]) {  // precision replays still in flight
+                for (int b = 0; b <= o.bounces; ++b) bounce();
+                CR_CUDA(cudaMemcpyAsync(g.hostCounts, g.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                CR_CUDA(cudaStreamSynchronize(s));
+                if (g.hostCounts[cur]) throw crh::Error(CR_ERR_DEVICE_TIMEOUT, "paths still live after the bounce limit");
+            }
+            k_accumulate<<<g.gridSmall, 128, 0, s>>>(g.st, w, g.acc);
+            ++launches;
+            if (perSample) {
+                float* dst = nullptr;
+                const size_t bytes = static_cast<size_t>(3) * total * sizeof(float);
+                (void)bytes;
+                // stage through the film buffer of the wave's own size
+                float* stage = nullptr;
+                CR_CUDA(cudaMallocAsync(&stage, static_cast<size_t>(3) * pixels * ns * sizeof(float), s));
+                WaveInfo wl = w;
+                wl.sample0 = 0;  // stage is indexed from the wave's first sample
+                k_dump_samples<<<g.gridSmall, 128, 0, s>>>(g.st, wl, pixels, stage);
+                for (uint32_t k = 0; k < ns; ++k) {
+                    dst = perSample + 3 * (static_cast<uint64_t>(s0 + k) * pixels + p0);
+                    CR_CUDA(cudaMemcpyAsync(dst, stage + 3 * (static_cast<uint64_t>(k) * pixels + p0),
+                                            static_cast<size_t>(3) * w.npix * sizeof(float), cudaMemcpyDeviceToHost, s));
+                }
+                CR_CUDA(cudaFreeAsync(stage, s));
+            }
+            CR_CUDA(cudaMemcpyAsync(g.hostStats, g.stats, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaStreamSynchronize(s));
+            CR_CUDA(cudaGetLastError());
+            for (auto& te : timed) {
+                float ms = 0;
+                CR_CUDA(cudaEventElapsedTime(&ms, g.event(te.first), g.event(te.first + 1)));
+                (te.second == 0 ? extendMs : te.second == 1 ? shadeMs : shadowMs) += ms;
+            }
+            if (g.hostStats[kStatErrorKey] != ~0ull) errored = true;
+            done += static_cast<uint64_t>(w.paths);
+            if (progress) {
+                const auto now = std::chrono::steady_clock::now();
+                if (now - lastProgress >= std::chrono::seconds(2)) {
+                    lastProgress = now;
+                    progress(done, total, std::chrono::duration<double>(now - start).count(), user);
+                }
+            }
+        }
+    }
+    if (errored) {
+        // Re-run the first failing sample alone to recover the reference's message.
+        const unsigned long long key = g.hostStats[kStatErrorKey];
+        const uint32_t sample = static_cast<uint32_t>(key & ((1ull << 21) - 1));
+        const uint64_t rank = key >> 21;
+        const uint64_t tilesX = (static_cast<uint64_t>(o.width) + 15) / 16;
+        const uint64_t tile = rank / 256, within = rank % 256;
+        const uint32_t x = static_cast<uint32_t>((tile % tilesX) * 16 + within % 16);
+        const uint32_t y = static_cast<uint32_t>((tile / tilesX) * 16 + within / 16);
+        DevError host{};
+        CR_CUDA(cudaMemsetAsync(g.detail, 0, sizeof(DevError), s));
+        CR_CUDA(cudaMemsetAsync(g.stats, 0, 2 * sizeof(unsigned long long), s));
+        k_trace_one<<<1, 32, 0, s>>>(g.dev, P, g.st, y * static_cast<uint32_t>(o.width) + x, sample, g.detail, g.stats, g.stats + 1);
+        CR_CUDA(cudaMemcpyAsync(&host, g.detail, sizeof(DevError), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        if (!host.code) { host.code = -1; host.x = static_cast<int32_t>(x); host.y = static_cast<int32_t>(y); host.sample = static_cast<int32_t>(sample); }
+        if (host.code == kErrStackOverflow) throw crh::Error(CR_ERR_RENDER, crh::sample_error_message(host));
+        throw crh::Error(CR_ERR_RENDER, crh::sample_error_message(host));
+    }
+    k_film<<<g.gridSmall, 128, 0, s>>>(g.acc, g.film, pixels, o.samples);
+    ++launches;
+    CR_CUDA(cudaEventRecord(t1, s));
+    if (filmHost) CR_CUDA(cudaMemcpyAsync(filmHost, g.film, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    CR_CUDA(cudaGetLastError());
+    float deviceMs = 0;
+    CR_CUDA(cudaEventElapsedTime(&deviceMs, t0, t1));
+    const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->seconds = seconds;
+        stats->device_ms = deviceMs;
+        stats->extend_ms = extendMs; stats->shade_ms = shadeMs; stats->shadow_ms = shadowMs;
+        stats->workers = referenceWorkers(o);
+        stats->waves = waves;
+        stats->camera_samples = total;
+        stats->boundary_retries = g.hostStats[kStatRetries];
+        stats->extend_rays = g.hostStats[kStatExtendRays];
+        stats->shadow_rays = g.hostStats[kStatShadowRays];
+        stats->kernel_launches = launches;
+    }
+    if (progress) progress(total, total, seconds, user);
+}
+
+cr_gpu_tuning defaults(const cr_gpu_tuning* t) {
+    cr_gpu_tuning d{};
+    if (t) d = *t;
+    return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+cr_status cr_gpu_device_count(int* count) {
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) { n = 0; cudaGetLastError(); }
+    if (count) *count = n;
+    return CR_OK;
+}
+
+cr_status cr_gpu_scene_create(const cr_scene_desc* scene, const cr_environment_desc* environment, int device, cr_gpu_scene** out) {
+    try {
+        if (!scene || !out) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "scene or out is NULL");
+        *out = nullptr;
+        cr_environment_desc black{};
+        const cr_environment_desc& env = environment ? *environment : black;
+        auto g = std::make_unique<cr_gpu_scene>();
+        g->device = device;
+        CR_CUDA(cudaSetDevice(device));
+        CR_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        uploadScene(*g, *scene, env);
+        *out = g.release();
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_scene_destroy(cr_gpu_scene* scene) {
+    delete scene;
+    return CR_OK;
+}
+
+cr_status cr_gpu_scene_bytes(const cr_gpu_scene* scene, uint64_t* bytes) {
+    if (!scene || !bytes) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "scene or bytes is NULL");
+    *bytes = scene->geometry.bytes + scene->work.bytes + scene->filmAlloc.bytes;
+    return CR_OK;
+}
+
+cr_status cr_gpu_intersect(cr_gpu_scene* g, const cr_ray* rays, uint64_t count, int any, uint32_t ignore,
+                           cr_hit* hits, uint8_t* found, const cr_gpu_tuning* tuning) {
+    try {
+        if (!g) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "scene is NULL");
+        if (count == 0) return CR_OK;
+        if (!rays || !hits || !found) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "rays, hits or found is NULL");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        const cr_gpu_tuning t = defaults(tuning);
+        CR_CUDA(cudaSetDevice(g->device));
+        cudaStream_t s = g->stream;
+        DevAlloc tmp;
+        cr_ray* dr = tmp.upload(rays, count, s);
+        cr_hit* dh = tmp.upload(hits, count, s);
+        uint8_t* df = tmp.alloc<uint8_t>(count);
+        unsigned long long* de = tmp.alloc<unsigned long long>(1);
+        const unsigned long long none = ~0ull;
+        CR_CUDA(cudaMemcpyAsync(de, &none, sizeof(none), cudaMemcpyHostToDevice, s));
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+        k_intersect_batch<<<sms * 8, 128, 0, s>>>(g->dev, dr, dh, df, count, any, ignore, t.exact_traversal, de);
+        CR_CUDA(cudaGetLastError());
+        unsigned long long errIndex = 0;
+        CR_CUDA(cudaMemcpyAsync(hits, dh, count * sizeof(cr_hit), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaMemcpyAsync(found, df, count, cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaMemcpyAsync(&errIndex, de, sizeof(errIndex), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        tmp.release();
+        if (errIndex != ~0ull) return crh::set_last_error(CR_ERR_LOGIC, "BVH traversal exceeded its bounded stack");
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_camera_rays(cr_gpu_scene* g, const cr_camera* camera, const cr_render_options* options, uint32_t sample, cr_ray* rays) {
+    try {
+        if (!g || !camera || !options || !rays) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        crh::validate_options(*options);
+        const cr_gpu_tuning t{};
+        RenderParams P = makeParams(*g, *camera, *options, t);
+        CR_CUDA(cudaSetDevice(g->device));
+        cudaStream_t s = g->stream;
+        const uint64_t pixels = static_cast<uint64_t>(options->width) * options->height;
+        DevAlloc tmp;
+        cr_ray* dr = tmp.alloc<cr_ray>(pixels);
+        unsigned long long* de = tmp.alloc<unsigned long long>(1);
+        const unsigned long long none = ~0ull;
+        CR_CUDA(cudaMemcpyAsync(de, &none, sizeof(none), cudaMemcpyHostToDevice, s));
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+        k_camera_rays<<<sms * 8, 128, 0, s>>>(P, sample, dr, de);
+        CR_CUDA(cudaGetLastError());
+        unsigned long long key = 0;
+        CR_CUDA(cudaMemcpyAsync(rays, dr, pixels * sizeof(cr_ray), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaMemcpyAsync(&key, de, sizeof(key), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        tmp.release();
+        if (key != ~0ull) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "Unrepresentable perspective ray");
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_render(cr_gpu_scene* g, const cr_camera* camera, const cr_render_options* options, cr_progress_fn progress,
+                        void* user, float* film_rgb, cr_render_stats* stats, const cr_gpu_tuning* tuning) {
+    try {
+        if (!g || !camera || !options) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        renderImpl(*g, *camera, *options, progress, user, film_rgb, stats, defaults(tuning), nullptr);
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_render_resident(cr_gpu_scene* g, const cr_camera* camera, const cr_render_options* options,
+                                 cr_render_stats* stats, const cr_gpu_tuning* tuning, float* per_sample_rgb) {
+    try {
+        if (!g || !camera || !options) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        renderImpl(*g, *camera, *options, nullptr, nullptr, nullptr, stats, defaults(tuning), per_sample_rgb);
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_film_download(cr_gpu_scene* g, float* film_rgb, uint64_t floats) {
+    try {
+        if (!g || !film_rgb) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        if (floats > 3 * g->filmPixels) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "film request larger than the last render");
+        CR_CUDA(cudaSetDevice(g->device));
+        CR_CUDA(cudaMemcpyAsync(film_rgb, g->film, floats * sizeof(float), cudaMemcpyDeviceToHost, g->stream));
+        CR_CUDA(cudaStreamSynchronize(g->stream));
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+}  // extern "C"

@@ -1,0 +1,237 @@
+"""Seeded synthetic scenes for the two plain-tracer workloads.
+
+room_scene          256x256, 16 spp, 8 bounces: a closed 2x2x2 room of 10 inward quads (20
+                    triangles), two 0.4x0.4 emitter quads of radiance 15 (4 triangles) and 64
+                    random triangles (edges 0.05-0.4), 70% GGX conductors (roughness U[0.05,1],
+                    albedo U[0.2,0.9]^3, two-sided) and 30% thin smooth dielectrics (IOR 1.5).
+                    No environment. 88 triangles.
+
+sphere_grid_scene   1920x1080, 64 spp, 16 bounces: 20x20 closed, radially displaced spheres
+                    (77 slices x 18 stacks = 2,618 triangles each, displacement amplitude 0.1)
+                    over a 16x43-quad ground grid (1,376 triangles): 1,048,576 triangles in
+                    total. Half the spheres are GGX conductors (roughness U[0.02,0.6]), half are
+                    smooth closed dielectrics (IOR U[1.3,1.7]). A 2048x1024 RGB equirect sky of
+                    log-normal (mu=0, sigma=1) texels plus a 0.5-degree sun disk of radiance 5e4.
+
+All draws come from numpy's PCG64 with fixed seeds, so every call returns identical arrays.
+Triangles are returned un-finalized (Scene::finalize computes areas and normals).
+"""
+import math
+
+import numpy as np
+
+from crgpu import Camera, Options, new_materials, new_triangles
+
+ROOM_SEED = 0x5EED0001
+GRID_SEED = 0x5EED0002
+
+
+def _quad(tris, a, b, c, d, material, inward=None):
+    """Two triangles (a,b,c), (a,c,d), wound so that cross(b-a, c-a) points along `inward`."""
+    a, b, c, d = (np.asarray(p, np.float32) for p in (a, b, c, d))
+    n = np.cross(b - a, c - a)
+    if inward is not None and np.dot(n, inward) < 0:
+        b, d = d, b
+        n = -n
+    n = (n / np.linalg.norm(n)).astype(np.float32)
+    for verts, uvs in (((a, b, c), ((0, 0), (1, 0), (1, 1))), ((a, c, d), ((0, 0), (1, 1), (0, 1)))):
+        t = new_triangles(1)[0]
+        for k in range(3):
+            t["v"][k]["position"] = verts[k]
+            t["v"][k]["normal"] = n
+            t["v"][k]["uv"][0] = uvs[k]
+            t["v"][k]["uv"][1] = uvs[k]
+        t["material"] = material
+        tris.append(t)
+
+
+def room_scene(seed=ROOM_SEED):
+    """Returns dict(triangles, materials, camera, options, env=None)."""
+    rng = np.random.default_rng(seed)
+    mats = new_materials(4)
+    # 0 white walls, 1 red wall, 2 green wall, 3 emitter; random triangles get their own.
+    for i, col in enumerate(((0.75, 0.75, 0.75), (0.7, 0.2, 0.15), (0.2, 0.6, 0.2))):
+        mats[i]["base_color"][:3] = col
+        mats[i]["metallic"] = 0.0
+        mats[i]["roughness"] = 1.0
+    mats[3]["base_color"][:3] = 0.0
+    mats[3]["metallic"] = 0.0
+    mats[3]["emission"] = 15.0
+    tris = []
+    lo, hi = -1.0, 1.0
+    # floor, ceiling, left, right: two quads each (split at z=0); back and front: one each.
+    for z0, z1 in ((lo, 0.0), (0.0, hi)):
+        _quad(tris, (lo, 0, z0), (hi, 0, z0), (hi, 0, z1), (lo, 0, z1), 0, inward=(0, 1, 0))
+        _quad(tris, (lo, 2, z0), (hi, 2, z0), (hi, 2, z1), (lo, 2, z1), 0, inward=(0, -1, 0))
+        _quad(tris, (lo, 0, z0), (lo, 2, z0), (lo, 2, z1), (lo, 0, z1), 1, inward=(1, 0, 0))
+        _quad(tris, (hi, 0, z0), (hi, 2, z0), (hi, 2, z1), (hi, 0, z1), 2, inward=(-1, 0, 0))
+    _quad(tris, (lo, 0, lo), (hi, 0, lo), (hi, 2, lo), (lo, 2, lo), 0, inward=(0, 0, 1))
+    _quad(tris, (lo, 0, hi), (hi, 0, hi), (hi, 2, hi), (lo, 2, hi), 0, inward=(0, 0, -1))
+    # two 0.4 x 0.4 emitters just below the ceiling, facing down
+    for cx in (-0.45, 0.45):
+        y = 1.995
+        _quad(tris, (cx - 0.2, y, -0.2), (cx + 0.2, y, -0.2), (cx + 0.2, y, 0.2), (cx - 0.2, y, 0.2), 3, inward=(0, -1, 0))
+    # 64 random triangles inside the room
+    extra = []
+    ilo = np.array([-0.9, 0.1, -0.9]); ihi = np.array([0.9, 1.9, 0.9])
+    while len(extra) < 64:
+        v0 = rng.uniform(ilo, ihi)
+        dirs = rng.normal(size=(2, 3))
+        dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+        lens = rng.uniform(0.05, 0.4, size=2)
+        v1 = v0 + lens[0] * dirs[0]
+        v2 = v0 + lens[1] * dirs[1]
+        e = np.linalg.norm(v2 - v1)
+        area = 0.5 * np.linalg.norm(np.cross(v1 - v0, v2 - v0))
+        inside = np.all((np.stack([v1, v2]) > ilo) & (np.stack([v1, v2]) < ihi))
+        if not (0.05 <= e <= 0.4) or area < 1e-4 or not inside:
+            continue
+        extra.append((v0, v1, v2))
+    rand_mats = new_materials(64)
+    kinds = rng.uniform(size=64) < 0.7
+    for i in range(64):
+        m = rand_mats[i]
+        m["double_sided"] = 1
+        if kinds[i]:  # GGX conductor
+            m["metallic"] = 1.0
+            m["roughness"] = rng.uniform(0.05, 1.0)
+            m["base_color"][:3] = rng.uniform(0.2, 0.9, size=3)
+        else:  # thin smooth dielectric
+            m["metallic"] = 0.0
+            m["transmission"] = 1.0
+            m["ior"] = 1.5
+            m["roughness"] = 0.0
+            m["thickness"] = 0.0
+            m["base_color"][:3] = 1.0
+    for i, (v0, v1, v2) in enumerate(extra):
+        t = new_triangles(1)[0]
+        for k, p in enumerate((v0, v1, v2)):
+            t["v"][k]["position"] = p.astype(np.float32)
+        t["material"] = 4 + i
+        tris.append(t)
+    materials = np.concatenate([mats, rand_mats])
+    triangles = np.array(tris, dtype=tris[0].dtype)
+    camera = Camera.make(position=(0, 1, 0.98), forward=(0, 0, -1), right=(1, 0, 0), up=(0, 1, 0),
+                         yfov=math.radians(60.0))
+    options = Options.make(width=256, height=256, samples=16, bounces=8, threads=0, seed=42)
+    return dict(triangles=triangles, materials=materials, lights=None, camera=camera, options=options, env=None,
+                name="room-88tri-256x256-16spp-d8")
+
+
+def _sphere_mesh(slices=77, stacks=18):
+    """Unit lat-long sphere: poles plus (stacks-1) rings; 2*slices*(stacks-1) outward triangles."""
+    rings = []
+    for i in range(1, stacks):
+        th = math.pi * i / stacks
+        for j in range(slices):
+            ph = 2 * math.pi * j / slices
+            rings.append((math.sin(th) * math.cos(ph), math.cos(th), math.sin(th) * math.sin(ph)))
+    verts = np.array([(0.0, 1.0, 0.0)] + rings + [(0.0, -1.0, 0.0)], np.float64)
+    top, bottom = 0, len(verts) - 1
+    ring = lambda i, j: 1 + (i * slices) + (j % slices)
+    faces = []
+    for j in range(slices):
+        faces.append((top, ring(0, j + 1), ring(0, j)))
+    for i in range(stacks - 2):
+        for j in range(slices):
+            a, b = ring(i, j), ring(i, j + 1)
+            c, d = ring(i + 1, j), ring(i + 1, j + 1)
+            faces.append((a, b, d))
+            faces.append((a, d, c))
+    for j in range(slices):
+        faces.append((bottom, ring(stacks - 2, j), ring(stacks - 2, j + 1)))
+    faces = np.array(faces, np.int64)
+    # orient outward
+    p = verts[faces]
+    n = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+    flip = np.einsum("ij,ij->i", n, p.mean(axis=1)) < 0
+    faces[flip] = faces[flip][:, [0, 2, 1]]
+    return verts, faces
+
+
+def sky_image(width=2048, height=1024, seed=GRID_SEED + 1, sun_elevation_deg=35.0, sun_azimuth_deg=60.0,
+              sun_diameter_deg=0.5, sun_radiance=5e4):
+    """RGBA float32 (H, W, 4): log-normal(0, 1) grey texels and a sun disk."""
+    rng = np.random.default_rng(seed)
+    img = np.ones((height, width, 4), np.float32)
+    img[..., :3] = np.exp(rng.normal(0.0, 1.0, size=(height, width, 1))).astype(np.float32)
+    theta = (np.arange(height) + 0.5) / height * math.pi
+    phi = ((np.arange(width) + 0.5) / width - 0.5) * 2 * math.pi
+    st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
+    d = np.stack([st * np.cos(phi)[None, :], np.broadcast_to(ct, (height, width)), st * np.sin(phi)[None, :]], -1)
+    el, az = math.radians(sun_elevation_deg), math.radians(sun_azimuth_deg)
+    sun = np.array([math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az)])
+    inside = d @ sun >= math.cos(math.radians(sun_diameter_deg / 2))
+    img[inside, :3] = sun_radiance
+    return img
+
+
+def sphere_grid_scene(seed=GRID_SEED, width=1920, height=1080, samples=64, bounces=16, sky=True):
+    """Returns dict(triangles, materials, camera, options, env_image)."""
+    rng = np.random.default_rng(seed)
+    unit, faces = _sphere_mesh()
+    grid, spacing, radius, amp = 20, 1.1, 0.38, 0.1
+    mats = new_materials(grid * grid + 1)
+    ground = grid * grid
+    mats[ground]["metallic"] = 0.0
+    mats[ground]["roughness"] = 0.8
+    mats[ground]["base_color"][:3] = 0.5
+    kinds = rng.uniform(size=grid * grid) < 0.5
+    tri_blocks = []
+    for k in range(grid * grid):
+        i, j = divmod(k, grid)
+        m = mats[k]
+        if kinds[k]:
+            m["metallic"] = 1.0
+            m["roughness"] = rng.uniform(0.02, 0.6)
+            m["base_color"][:3] = rng.uniform(0.3, 0.95, size=3)
+        else:
+            m["metallic"] = 0.0
+            m["transmission"] = 1.0
+            m["ior"] = rng.uniform(1.3, 1.7)
+            m["roughness"] = 0.0
+            m["thickness"] = 1.0
+            m["base_color"][:3] = 1.0
+        ph = rng.uniform(0, 2 * math.pi, size=3)
+        fr = rng.uniform(2.0, 4.0, size=3)
+        noise = np.sin(fr[0] * unit[:, 0] + ph[0]) * np.sin(fr[1] * unit[:, 1] + ph[1]) * np.sin(fr[2] * unit[:, 2] + ph[2])
+        r = radius + amp * noise
+        center = np.array([(i - (grid - 1) / 2) * spacing, radius + amp, (j - (grid - 1) / 2) * spacing])
+        verts = unit * r[:, None] + center
+        # smooth vertex normals: area-weighted face normals
+        p = verts[faces]
+        fn = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+        vn = np.zeros_like(verts)
+        for c in range(3):
+            np.add.at(vn, faces[:, c], fn)
+        vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+        t = new_triangles(len(faces))
+        t["v"]["position"] = verts[faces].astype(np.float32)
+        t["v"]["normal"] = vn[faces].astype(np.float32)
+        t["material"] = k
+        tri_blocks.append(t)
+    # ground grid: 16 x 43 quads over the sphere footprint
+    nx, nz = 16, 43
+    ext = grid * spacing / 2 + 1.0
+    xs = np.linspace(-ext, ext, nx + 1)
+    zs = np.linspace(-ext, ext, nz + 1)
+    g = new_triangles(2 * nx * nz)
+    q = 0
+    for a in range(nx):
+        for b in range(nz):
+            p00 = (xs[a], 0.0, zs[b]); p10 = (xs[a + 1], 0.0, zs[b])
+            p11 = (xs[a + 1], 0.0, zs[b + 1]); p01 = (xs[a], 0.0, zs[b + 1])
+            for tri in ((p00, p01, p11), (p00, p11, p10)):  # cross(b-a, c-a) = +y
+                g[q]["v"]["position"] = np.array(tri, np.float32)
+                g[q]["v"]["normal"] = (0.0, 1.0, 0.0)
+                g[q]["material"] = ground
+                q += 1
+    tri_blocks.append(g)
+    triangles = np.concatenate(tri_blocks)
+    assert len(triangles) == 1 << 20
+    camera = Camera.make(position=(0.0, 6.0, 17.0), forward=(0.0, -6.0, -17.0), right=(1, 0, 0), up=(0, 1, 0),
+                         yfov=math.radians(40.0))
+    options = Options.make(width=width, height=height, samples=samples, bounces=bounces, threads=0, seed=42)
+    return dict(triangles=triangles, materials=mats, lights=None, camera=camera, options=options,
+                env_image=sky_image() if sky else None,
+                name="sphere-grid-1M-1920x1080-64spp-d16")

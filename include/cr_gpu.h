@@ -1,0 +1,291 @@
+/*
+ * cr_gpu.h — C ABI of the B200 path-tracing backend.
+ *
+ * This is the drop-in boundary for CPU-Renderer's per-path radiance loop. It replaces,
+ * behind a plain C interface (no C++ or torch types), these reference entry points:
+ *
+ *   cr::render(scene, bvh, camera, environment, options, progress)   src/render.h:53
+ *   cr::Bvh::intersect(scene, ray, hit, any, ignoreTriangle)          src/scene.h:126-127
+ *   cr::RenderOptions::validate()                                     src/render.h:38, render.cpp:97-104
+ *   cr::Bvh::build(scene)  (host restatement, same node array)        src/scene.h:123, geometry.cpp:463-550
+ *   cr::Scene::finalize()  (host restatement)                         src/scene.h:232, geometry.cpp:296-397
+ *   cr::Camera::generate(...)                                         src/scene.h:206, geometry.cpp:213-234
+ *
+ * All structs below are plain data. The first five mirror the reference's value types
+ * field for field, so a C++ caller holding cr::Triangle / cr::Ray / cr::Hit arrays can
+ * pass them without conversion (the C++ drop-in shim static_asserts the layouts).
+ *
+ * Ownership: the library never retains a caller pointer past the call that received it.
+ * A cr_gpu_scene owns device copies of everything it needs.
+ *
+ * Errors: every entry point returns a cr_status. The text of the most recent failure on
+ * the calling thread is available from cr_gpu_last_error(); for a failed sample it has
+ * the reference's form "Pixel (x,y), sample s: <cause>" (render.cpp:437-438).
+ */
+#ifndef CR_GPU_H
+#define CR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CR_GPU_ABI_VERSION 1
+
+typedef enum cr_status {
+    CR_OK = 0,
+    CR_ERR_INVALID_ARGUMENT = 1, /* bad options/scene/camera: std::runtime_error / invalid_argument */
+    CR_ERR_RENDER = 2,           /* a camera sample failed; message carries pixel and sample   */
+    CR_ERR_OUT_OF_RANGE = 3,     /* index outside its table (std::out_of_range)               */
+    CR_ERR_LENGTH = 4,           /* too many triangles for 32-bit node indices (length_error) */
+    CR_ERR_LOGIC = 5,            /* traversal stack exhausted (std::logic_error)              */
+    CR_ERR_OUT_OF_MEMORY = 6,    /* device or host allocation failed                          */
+    CR_ERR_DEVICE_TIMEOUT = 7,   /* a bounded device loop gave up                              */
+    CR_ERR_CUDA = 8,             /* CUDA runtime failure                                      */
+    CR_ERR_UNSUPPORTED = 9       /* input uses a feature this build does not implement        */
+} cr_status;
+
+/* cr::Vertex (scene.h:155): position, normal, tangent (w = handedness), two UV sets. 56 bytes. */
+typedef struct cr_vertex {
+    float position[3];
+    float normal[3];
+    float tangent[4];
+    float uv[2][2];
+} cr_vertex;
+
+/* cr::Triangle (scene.h:158-163) after Scene::finalize(): world-space vertices, material
+ * index, outward geometric normal and area. 188 bytes. */
+typedef struct cr_triangle {
+    cr_vertex v[3];
+    uint32_t material;
+    float geometric_normal[3];
+    float area;
+} cr_triangle;
+
+/* cr::Ray (scene.h:139-143): origin + origin_low + t*direction on [tmin, tmax]. 44 bytes. */
+typedef struct cr_ray {
+    float origin[3];
+    float direction[3];
+    float tmin, tmax;
+    float origin_low[3];
+} cr_ray;
+
+/* cr::Hit (scene.h:166): double t, u, v and the triangle index. 32 bytes. */
+typedef struct cr_hit {
+    double t, u, v;
+    uint32_t triangle;
+    uint32_t reserved_;
+} cr_hit;
+
+/* Bvh::Node (scene.h:261): bounds, then first/count; count > 0 is a leaf over
+ * indices[first, first+count), count == 0 an interior node whose children are the two
+ * adjacent nodes first and first+1. 32 bytes. */
+typedef struct cr_bvh_node {
+    float lo[3];
+    float hi[3];
+    uint32_t first;
+    uint32_t count;
+} cr_bvh_node;
+
+/* cr::TextureSlot (scene.h:179-182). texture == -1 means "no map". */
+typedef struct cr_texture_slot {
+    int32_t texture;
+    int32_t texcoord;
+    float offset[2];
+    float scale[2];
+    float rotation;
+} cr_texture_slot;
+
+enum { CR_WRAP_REPEAT = 0, CR_WRAP_CLAMP = 1, CR_WRAP_MIRROR = 2 };
+enum { CR_ALPHA_OPAQUE = 0, CR_ALPHA_MASK = 1 };
+
+/* cr::Material (scene.h:187-199) without its name. */
+typedef struct cr_material {
+    float base_color[4];
+    float metallic, roughness;
+    float emission[3];
+    float transmission, ior;
+    float thickness, attenuation_distance;
+    float attenuation_color[3];
+    int32_t double_sided;
+    int32_t alpha_mode;
+    float alpha_cutoff, normal_scale;
+    cr_texture_slot base_color_texture;
+    cr_texture_slot metallic_roughness_texture;
+    cr_texture_slot normal_texture;
+    cr_texture_slot emissive_texture;
+    cr_texture_slot transmission_texture;
+} cr_material;
+
+/* cr::Image (scene.h:176): width*height RGBA float texels, row-major, top row first. */
+typedef struct cr_image {
+    int32_t width, height;
+    const float* pixels;
+} cr_image;
+
+/* cr::Texture (scene.h:177). */
+typedef struct cr_texture {
+    int32_t image;
+    int32_t wrap_s, wrap_t;
+    int32_t linear;
+} cr_texture;
+
+enum { CR_LIGHT_POINT = 0, CR_LIGHT_DIRECTIONAL = 1, CR_LIGHT_SPOT = 2 };
+
+/* cr::PunctualLight (scene.h:211-215). */
+typedef struct cr_punctual_light {
+    int32_t type;
+    float position[3];
+    float direction[3];
+    float color[3];
+    float intensity, range, inner_cone, outer_cone;
+} cr_punctual_light;
+
+/* cr::Camera (scene.h:202-207) without its name. */
+typedef struct cr_camera {
+    float position[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float yfov, aspect, near_clip, far_clip;
+} cr_camera;
+
+/* cr::RenderOptions (render.h:31-39). */
+typedef struct cr_render_options {
+    int32_t width, height, samples, bounces, threads;
+    uint64_t seed;
+    int32_t next_event_estimation, russian_roulette;
+} cr_render_options;
+
+/* Everything a scene upload needs. triangles must already be finalized (Scene::finalize()).
+ * bvh_nodes/bvh_indices may be NULL, in which case the library builds the reference's
+ * binned-SAH tree itself (cr_bvh_build). */
+typedef struct cr_scene_desc {
+    const cr_triangle* triangles;
+    uint64_t triangle_count;
+    const cr_material* materials;
+    uint32_t material_count;
+    const cr_punctual_light* lights;
+    uint32_t light_count;
+    const cr_image* images;
+    uint32_t image_count;
+    const cr_texture* textures;
+    uint32_t texture_count;
+    const cr_bvh_node* bvh_nodes;
+    uint64_t bvh_node_count;
+    const uint32_t* bvh_indices;
+    uint64_t bvh_index_count;
+} cr_scene_desc;
+
+/* cr::Environment (render.h:8-28). With pixels == NULL it is the constant radiance
+ * `constant`. Otherwise a width*height RGBA equirect image; rotation_radians is the
+ * already-reduced yaw the reference stores (fmod(degrees,360)*pi/180, render.cpp:24;
+ * cr_environment_rotation() computes it). cdf may be NULL (the library rebuilds the
+ * reference's FP64 CDF, render.cpp:28-41) or the caller's copy of it. */
+typedef struct cr_environment_desc {
+    float constant[3];
+    const float* pixels;
+    int32_t width, height;
+    float rotation_radians;
+    float intensity;
+    const double* cdf;
+} cr_environment_desc;
+
+/* Per-render report; mirrors cr::RenderResult (render.h:41-48) plus device figures. */
+typedef struct cr_render_stats {
+    double seconds;             /* wall time of the call, like RenderResult::seconds    */
+    double device_ms;           /* CUDA-event time of all render kernels                 */
+    double extend_ms;           /* CUDA-event time of the closest-hit launches          */
+    double shadow_ms;           /* CUDA-event time of the any-hit launches              */
+    double shade_ms;            /* CUDA-event time of the shading launches              */
+    int32_t workers;            /* the reference's worker-count formula (render.cpp:363) */
+    int32_t waves;              /* sample waves launched                                 */
+    uint64_t camera_samples;    /* width*height*samples                                  */
+    uint64_t boundary_retries;  /* precision replays (render.cpp:409)                    */
+    uint64_t extend_rays;       /* closest-hit rays traced                               */
+    uint64_t shadow_rays;       /* any-hit rays traced                                   */
+    uint64_t kernel_launches;   /* kernels launched by this call                         */
+} cr_render_stats;
+
+typedef void (*cr_progress_fn)(uint64_t complete, uint64_t total, double seconds, void* user);
+
+/* Render-time switches that have no counterpart in cr::RenderOptions. Zero-initialise for
+ * the defaults. */
+typedef struct cr_gpu_tuning {
+    int32_t exact_traversal;   /* 1: FP64 box tests in the reference's order for every ray */
+    int32_t env_alias;         /* 1: alias-table environment sampling (different streams)   */
+    int32_t paths_per_wave;    /* 0: automatic                                             */
+    int32_t block_size;        /* 0: automatic                                             */
+    int32_t use_graphs;        /* 0: automatic (on), -1: off                               */
+    int32_t time_phases;       /* 1: CUDA-event time every extend/shade/shadow launch      */
+} cr_gpu_tuning;
+
+typedef struct cr_gpu_scene cr_gpu_scene;
+
+/* ---- library ---------------------------------------------------------------------- */
+int cr_gpu_abi_version(void);
+/* Copies the last error text of this thread into buf (always NUL-terminated when n>0);
+ * returns its full length. */
+size_t cr_gpu_last_error(char* buf, size_t n);
+cr_status cr_gpu_device_count(int* count);
+
+/* ---- host-side restatements of the reference's preparation steps ------------------- */
+/* RenderOptions::validate (render.cpp:97-104). */
+cr_status cr_options_validate(const cr_render_options* options);
+/* Scene::finalize (geometry.cpp:296-397) over the triangle array in place: validates,
+ * drops zero-area triangles (compacting the array and renumbering), fixes normals and
+ * tangents. *triangle_count is updated. Warnings are joined with '\n' into warnings
+ * (may be NULL). */
+cr_status cr_scene_finalize(cr_triangle* triangles, uint64_t* triangle_count,
+                            const cr_material* materials, uint32_t material_count,
+                            const cr_image* images, uint32_t image_count,
+                            const cr_texture* textures, uint32_t texture_count,
+                            char* warnings, size_t warnings_size);
+/* Bvh::build (geometry.cpp:463-550): nodes must hold 2*triangle_count-1 entries (at least
+ * one), indices triangle_count entries. *node_count receives the node count. */
+cr_status cr_bvh_build(const cr_triangle* triangles, uint64_t triangle_count,
+                       cr_bvh_node* nodes, uint64_t* node_count, uint32_t* indices);
+/* fmod(degrees, 360) * pi / 180 in float, as Environment's constructor stores it. */
+float cr_environment_rotation(float degrees);
+
+/* ---- device scene ------------------------------------------------------------------ */
+cr_status cr_gpu_scene_create(const cr_scene_desc* scene, const cr_environment_desc* environment,
+                              int device, cr_gpu_scene** out);
+cr_status cr_gpu_scene_destroy(cr_gpu_scene* scene);
+/* Device bytes held by the scene (geometry, BVH, environment, work buffers). */
+cr_status cr_gpu_scene_bytes(const cr_gpu_scene* scene, uint64_t* bytes);
+
+/* Bvh::intersect over a batch (scene.h:126-127): hits is read as the incoming Hit (its t
+ * is the upper bound, geometry.cpp:557) and overwritten where found[i] = 1; rays that
+ * find nothing keep their input hit, as the reference leaves Hit untouched. */
+cr_status cr_gpu_intersect(cr_gpu_scene* scene, const cr_ray* rays, uint64_t count, int any,
+                           uint32_t ignore_triangle, cr_hit* hits, uint8_t* found,
+                           const cr_gpu_tuning* tuning);
+
+/* Camera::generate for every pixel of one sample index, with the render's own jitter
+ * (two draws of the sample's stream, render.cpp:396-398). rays holds width*height. */
+cr_status cr_gpu_camera_rays(cr_gpu_scene* scene, const cr_camera* camera,
+                             const cr_render_options* options, uint32_t sample, cr_ray* rays);
+
+/* cr::render (render.cpp:352-456): film_rgb receives width*height linear RGB floats.
+ * progress may be NULL; it is called on this thread between sample waves, at most every
+ * two seconds, and once at the end. tuning may be NULL. */
+cr_status cr_gpu_render(cr_gpu_scene* scene, const cr_camera* camera,
+                        const cr_render_options* options, cr_progress_fn progress, void* user,
+                        float* film_rgb, cr_render_stats* stats, const cr_gpu_tuning* tuning);
+
+/* As cr_gpu_render, but the film stays in device memory (see cr_gpu_film_download).
+ * per_sample_rgb, when not NULL, receives samples*width*height*3 floats: the radiance of
+ * every camera sample (sample-major), for stream-level comparisons. */
+cr_status cr_gpu_render_resident(cr_gpu_scene* scene, const cr_camera* camera,
+                                 const cr_render_options* options, cr_render_stats* stats,
+                                 const cr_gpu_tuning* tuning, float* per_sample_rgb);
+cr_status cr_gpu_film_download(cr_gpu_scene* scene, float* film_rgb, uint64_t floats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CR_GPU_H */

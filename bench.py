@@ -1,0 +1,319 @@
+"""Benchmark of the plain GPU path tracer on the 1,048,576-triangle sphere-grid workload
+(1920x1080, 64 spp, 16 bounces, 2048x1024 sky with a 5e4 sun disk).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step renders the whole workload once (132.7 M camera samples). `value` is Msamples/s with
+the scene resident in HBM (CUDA-event time of the render's kernels, max over ranks); `e2e`
+is the same metric through the C ABI with host buffers: scene upload, render and film
+download every step. With --gpus N each rank renders its own replica (seed 42 + rank):
+weak scaling, no collective on the data path. `--impl reference` times the reference's
+own CPU renderer (built from its sources) on this host's cores instead.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cpu-renderer_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "Msamples/s"
+UNIT = "Msamples/s"
+WORKLOAD = "sphere-grid-1M-1920x1080-64spp-d16"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-spp", type=int, default=4)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(spp):
+    import crgpu
+    import workloads
+    sc = workloads.sphere_grid_scene(samples=spp)
+    tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
+    nodes, idx = crgpu.build_bvh(tris)
+    return sc, tris, nodes, idx
+
+
+def flush_l2(torch, device):
+    buf = torch.empty(64 << 20, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
+    buf.zero_()
+    torch.cuda.synchronize(device)
+    del buf
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return p.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per closest-hit ray from the committed ncu summary (profiles/), if any."""
+    path = os.path.join(ROOT, "profiles", "extend_sphere_grid.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f).get("dram_bytes_per_extend_ray")
+
+
+def cpu_reference_rate(sc, spp, threads):
+    """The reference's cr::render on this host's cores: Msamples/s on a bounded sample."""
+    import refimpl
+    if not refimpl.available():
+        return None
+    rs = refimpl.RefScene(sc["triangles"], sc["materials"]).build_bvh()
+    env = refimpl.RefEnvironment(image=sc["env_image"])
+    o = sc["options"]
+    import crgpu
+    opt = crgpu.Options.make(width=o.width, height=o.height, samples=spp, bounces=o.bounces, threads=threads, seed=o.seed)
+    film, st = rs.render(sc["camera"], opt, env)
+    return st["camera_samples"] / st["seconds"] / 1e6, st
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import refimpl
+    if not refimpl.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libcr_ref.so was not built"}))
+        return
+    threads = os.cpu_count() or 1
+    sc, _, _, _ = build_workload(args.spp)
+    rs = refimpl.RefScene(sc["triangles"], sc["materials"]).build_bvh()
+    env = refimpl.RefEnvironment(image=sc["env_image"])
+    import crgpu
+    o = sc["options"]
+    step_spp = 1  # one step: the full 1920x1080 frame at 1 spp of the same streams
+    opt = crgpu.Options.make(width=o.width, height=o.height, samples=step_spp, bounces=o.bounces, threads=threads, seed=o.seed)
+    for _ in range(args.warmup):
+        rs.render(sc["camera"], opt, env)
+    secs = []
+    for _ in range(args.steps):
+        _, st = rs.render(sc["camera"], opt, env)
+        secs.append(st["seconds"])
+    samples = o.width * o.height * step_spp
+    value = samples * len(secs) / sum(secs) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded procedural scene and sky)",
+        "config": {"workload": WORKLOAD, "triangles": 1 << 20, "width": o.width, "height": o.height, "spp": args.spp,
+                   "bounces": o.bounces, "step": f"{o.width}x{o.height} x {step_spp} spp of the same sample streams"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{o.width}x{o.height} x {step_spp} spp per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    import torch
+    import crgpu
+    distributed = world > 1
+    if distributed:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    sc, tris, nodes, idx = build_workload(args.spp)
+    cam, opt = sc["camera"], sc["options"]
+    opt.seed = 42 + rank
+    env = crgpu.env_desc(image=sc["env_image"])
+    g = crgpu.GpuScene(tris, sc["materials"], env=env, bvh=(nodes, idx), device=local)
+    samples_per_step = opt.width * opt.height * opt.samples
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if distributed:
+            torch.distributed.barrier()
+
+    # counting pass (untimed): node pairs and triangles per closest-hit ray
+    tc = crgpu.Tuning()
+    tc.count_traversal = 1
+    copt = crgpu.Options.make(width=opt.width, height=opt.height, samples=1, bounces=opt.bounces, seed=opt.seed)
+    cstats, _ = g.render_resident(cam, copt, tuning=tc)
+    pairs_per_ray = cstats["extend_pairs"] / max(1, cstats["extend_rays"])
+    tris_per_ray = cstats["extend_triangles"] / max(1, cstats["extend_rays"])
+
+    for _ in range(args.warmup):
+        g.render_resident(cam, opt)
+    # timed: device time of K renders; phase timing in a separate pass below
+    dev_ms, launches, ext_rays = [], 0, 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush_l2(torch, device)
+            barrier()
+            st, _ = g.render_resident(cam, opt)
+            barrier()
+            dev_ms.append(st["device_ms"])
+            launches += st["kernel_launches"]
+    total_ms = sum(dev_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    if distributed:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * samples_per_step * args.steps / (max_ms / 1e3) / 1e6
+
+    # dominant-kernel timing: one more render with CUDA events around every launch
+    tp = crgpu.Tuning()
+    tp.time_phases = 1
+    pst, _ = g.render_resident(cam, opt, tuning=tp)
+    ext_launches = pst["waves"] * (opt.bounces + 1)
+    bytes_per_ray = 64.0 * pairs_per_ray + 48.0 * tris_per_ray + 16 + 16 + 4 + 4 + 4 + 4
+    achieved = bytes_per_ray * pst["extend_rays"] / (pst["extend_ms"] / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic_per_ray = profile_traffic()
+    roofline = {
+        "kernel": "k_extend (closest hit)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "peak_source": peak_kind,
+        "traffic": (traffic_per_ray * pst["extend_rays"] / ext_launches) if traffic_per_ray else None,
+        "algorithmic_bytes_per_launch": bytes_per_ray * pst["extend_rays"] / ext_launches,
+        "bytes_per_ray": bytes_per_ray, "pairs_per_ray": pairs_per_ray, "triangles_per_ray": tris_per_ray,
+        "extend_ms_share": pst["extend_ms"] / pst["device_ms"],
+        "mrays_per_s": pst["extend_rays"] / (pst["extend_ms"] / 1e3) / 1e6,
+    }
+
+    # end to end through the C ABI with host buffers: upload, render, download every step
+    e2e_secs, h2d = [], 0
+    film = None
+    for _ in range(2):
+        barrier()
+        t0 = time.perf_counter()
+        ge = crgpu.GpuScene(tris, sc["materials"], env=env, bvh=(nodes, idx), device=local)
+        film, _ = ge.render(cam, opt)
+        h2d = ge.bytes()
+        ge.close()
+        barrier()
+        e2e_secs.append(time.perf_counter() - t0)
+    e2e_value = samples_per_step / min(e2e_secs) / 1e6 * world
+    h2d_bytes = int(tris.nbytes + nodes.nbytes + idx.nbytes + sc["env_image"].nbytes + sc["materials"].nbytes)
+    d2h_bytes = int(film.nbytes)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = cpu_reference_rate(sc, args.cpu_sample_spp, threads)
+        if r is not None:
+            cpu = {"value": r[0], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{opt.width}x{opt.height} x {args.cpu_sample_spp} spp of the same scene and streams "
+                             f"({r[1]['seconds']:.1f} s)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic (seeded procedural scene and sky)",
+            "config": {"workload": WORKLOAD, "triangles": int(len(tris)), "width": opt.width, "height": opt.height,
+                       "spp": opt.samples, "bounces": opt.bounces, "env": "2048x1024 log-normal + 0.5 deg sun 5e4",
+                       "parallelism": f"replicas x{world}", "l2": "256 MB buffer written between timed steps",
+                       "traversal": "fp32 conservative boxes + fp64 reference triangle test"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
+                    "note": "scene upload + render + film download per step through cr_gpu_* with host arrays"},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    g.close()
+    if distributed:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

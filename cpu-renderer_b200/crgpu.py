@@ -105,7 +105,8 @@ class Stats(C.Structure):
     _fields_ = [("seconds", C.c_double), ("device_ms", C.c_double), ("extend_ms", C.c_double),
                 ("shadow_ms", C.c_double), ("shade_ms", C.c_double), ("workers", C.c_int32), ("waves", C.c_int32),
                 ("camera_samples", C.c_uint64), ("boundary_retries", C.c_uint64), ("extend_rays", C.c_uint64),
-                ("shadow_rays", C.c_uint64), ("kernel_launches", C.c_uint64)]
+                ("shadow_rays", C.c_uint64), ("kernel_launches", C.c_uint64), ("extend_pairs", C.c_uint64),
+                ("extend_triangles", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -113,7 +114,8 @@ class Stats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("exact_traversal", C.c_int32), ("env_alias", C.c_int32), ("paths_per_wave", C.c_int32),
-                ("block_size", C.c_int32), ("use_graphs", C.c_int32), ("time_phases", C.c_int32)]
+                ("block_size", C.c_int32), ("use_graphs", C.c_int32), ("time_phases", C.c_int32),
+                ("count_traversal", C.c_int32)]
 
 
 class SceneDesc(C.Structure):
@@ -153,6 +155,7 @@ def _load():
         "cr_scene_finalize": (C.c_int, [P, C.POINTER(C.c_uint64), P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, C.c_char_p, C.c_size_t]),
         "cr_bvh_build": (C.c_int, [P, C.c_uint64, P, C.POINTER(C.c_uint64), P]),
         "cr_environment_rotation": (C.c_float, [C.c_float]),
+        "cr_environment_tables": (C.c_int, [C.POINTER(EnvDesc), P, P]),
         "cr_gpu_scene_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(EnvDesc), C.c_int, C.POINTER(P)]),
         "cr_gpu_scene_destroy": (C.c_int, [P]),
         "cr_gpu_scene_bytes": (C.c_int, [P, C.POINTER(C.c_uint64)]),

@@ -598,4 +598,16 @@ float cr_environment_rotation(float degrees) {  // render.cpp:24
     return std::fmod(degrees, 360.0f) * pi / 180;
 }
 
+cr_status cr_environment_tables(const cr_environment_desc* environment, double* cdf, double* weight_sum_integral) {
+    try {
+        if (!environment) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "environment is NULL");
+        crh::EnvTables t;
+        crh::build_environment(*environment, t);
+        if (cdf && !t.cdf.empty()) std::memcpy(cdf, t.cdf.data(), t.cdf.size() * sizeof(double));
+        if (weight_sum_integral) { weight_sum_integral[0] = t.weightSum; weight_sum_integral[1] = t.integral; }
+        return CR_OK;
+    } catch (const crh::Error& e) { return crh::set_last_error(e.status, e.what()); }
+    catch (const std::bad_alloc&) { return crh::set_last_error(CR_ERR_OUT_OF_MEMORY, "host allocation failed"); }
+}
+
 }  // extern "C"

@@ -32,7 +32,8 @@ struct WaveInfo {
     uint32_t pixel0, npix, sample0, nsamp, paths;
 };
 
-enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatWords = 4 };
+enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatPairs = 4, kStatTris = 5,
+       kStatWords = 6 };
 
 CR_D uint64_t errorKey(const RenderParams& P, uint32_t pixel, uint32_t sample) {
     const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
@@ -309,6 +310,7 @@ __global__ void k_generate(DevScene S, RenderParams P, PathSoA st, Queues q, Wav
     }
 }
 
+template <bool COUNT>
 __global__ void __launch_bounds__(128) k_extend(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, ErrSink E,
                                                 unsigned long long* stats) {
     const uint32_t n = q.counts[cur];
@@ -324,9 +326,15 @@ __global__ void __launch_bounds__(128) k_extend(DevScene S, RenderParams P, Path
         HitRec h;
         h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
         int err = 0;
-        const bool found = intersect<false>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0, h, err);
+        VisitCount vc;
+        const bool found = intersect<false, COUNT>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
+                                                   h, err, &vc);
         st.hit_tri[path] = found ? h.tri : kNoTriangle;
         if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+        if (COUNT) {
+            atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
+            atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
+        }
     }
 }
 
@@ -826,7 +834,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     cudaStream_t s = g.stream;
     const int block = tuning.block_size > 0 ? tuning.block_size : 128;
     if (!g.gridExtend) {
-        g.gridExtend = occupancyGrid(reinterpret_cast<const void*>(k_extend), 128, g.device);
+        g.gridExtend = occupancyGrid(reinterpret_cast<const void*>(k_extend<false>), 128, g.device);
         g.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade), 128, g.device);
         g.gridShadow = occupancyGrid(reinterpret_cast<const void*>(k_shadow), 128, g.device);
         int sms = 0;
@@ -870,7 +878,10 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     if (timePhases) { CR_CUDA(cudaEventRecord(g.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
                     ++launches;
                 };
-                rec(0, [&] { k_extend<<<g.gridExtend, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats); });
+                rec(0, [&] {
+                    if (tuning.count_traversal) k_extend<true><<<g.gridExtend, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats);
+                    else k_extend<false><<<g.gridExtend, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats);
+                });
                 rec(1, [&] { k_shade<<<g.gridShade, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats); });
                 rec(2, [&] { k_shadow<<<g.gridShadow, 128, 0, s>>>(g.dev, P, g.st, g.q, E, g.stats); });
                 cur ^= 1;
@@ -962,6 +973,8 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         stats->extend_rays = g.hostStats[kStatExtendRays];
         stats->shadow_rays = g.hostStats[kStatShadowRays];
         stats->kernel_launches = launches;
+        stats->extend_pairs = g.hostStats[kStatPairs];
+        stats->extend_triangles = g.hostStats[kStatTris];
     }
     if (progress) progress(total, total, seconds, user);
 }

@@ -99,9 +99,12 @@ CR_D void load_pair(const NodePair* pairs, uint32_t p, float4& a, float4& b, flo
 }
 
 // ---- exact traversal (geometry.cpp:554-639) ------------------------------------------------
-template <bool ANY>
+// Optional visit counters (node pairs fetched, triangles tested) for the roofline numerator.
+struct VisitCount { uint32_t pairs = 0, tris = 0; };
+
+template <bool ANY, bool COUNT = false>
 __device__ bool intersect_exact(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore,
-                                HitRec& hit, int& err) {
+                                HitRec& hit, int& err, VisitCount* vc = nullptr) {
     double closestLimit = smin(static_cast<double>(ray.tmax), hitT);
     float ctmax = smin(ray.tmax, next_up(static_cast<float>(closestLimit)));
     const float queryLimit = ctmax;
@@ -150,6 +153,7 @@ __device__ bool intersect_exact(const DevScene& S, const TRay& ray, double hitT,
         if (cnt) {
             for (uint32_t i = ref; i < ref + cnt; ++i) {
                 const float4 q0 = __ldg(S.tri_pos + 3 * static_cast<uint64_t>(i));
+                if (COUNT) ++vc->tris;
                 const uint32_t index = __float_as_uint(q0.w);
                 if (index == ignore) continue;
                 const float4 q1 = __ldg(S.tri_pos + 3 * static_cast<uint64_t>(i) + 1);
@@ -170,6 +174,7 @@ __device__ bool intersect_exact(const DevScene& S, const TRay& ray, double hitT,
         } else {
             float4 a, b, c; uint4 d;
             load_pair(S.pairs, ref, a, b, c, d);
+            if (COUNT) ++vc->pairs;
             float leftNear = 0, rightNear = 0;
             const bool left = box(a.x, a.y, a.z, a.w, b.x, b.y, leftNear);
             const bool right = box(b.z, b.w, c.x, c.y, c.z, c.w, rightNear);
@@ -197,14 +202,12 @@ __device__ bool intersect_exact(const DevScene& S, const TRay& ray, double hitT,
 // that underflow. Widening only ever adds boxes.
 constexpr float kBoxRel = 9.5367431640625e-07f;  // 2^-20
 constexpr float kBoxAbs = 1e-30f;
-// Zero direction components use +-1e30 instead of an infinite reciprocal, so an origin
-// lying exactly on a slab plane gives 0 (not 0*inf = NaN) and stays inside the slab.
-constexpr float kZeroDirInv = 1e30f;
 
 struct FastSetup {
     V3 o, inv;
     int kx, ky, kz;
     float Sx, Sy;
+    uint32_t zeroAxes;  // bit a set when direction component a is exactly zero
 };
 
 // Rays whose FP32 setup is well conditioned: no precise origin, and no direction component
@@ -222,9 +225,8 @@ CR_D bool fast_eligible(const TRay& r) {
 CR_D FastSetup fast_setup(const TRay& r) {
     FastSetup f;
     f.o = r.o;
-    f.inv = V3{r.d.x != 0 ? 1.0f / r.d.x : copysignf(kZeroDirInv, r.d.x),
-               r.d.y != 0 ? 1.0f / r.d.y : copysignf(kZeroDirInv, r.d.y),
-               r.d.z != 0 ? 1.0f / r.d.z : copysignf(kZeroDirInv, r.d.z)};
+    f.inv = V3{r.d.x != 0 ? 1.0f / r.d.x : 0.0f, r.d.y != 0 ? 1.0f / r.d.y : 0.0f, r.d.z != 0 ? 1.0f / r.d.z : 0.0f};
+    f.zeroAxes = (r.d.x == 0 ? 1u : 0u) | (r.d.y == 0 ? 2u : 0u) | (r.d.z == 0 ? 4u : 0u);
     int kz = 0;
     if (fabsf(r.d.y) > fabsf(r.d[kz])) kz = 1;
     if (fabsf(r.d.z) > fabsf(r.d[kz])) kz = 2;
@@ -236,14 +238,24 @@ CR_D FastSetup fast_setup(const TRay& r) {
     return f;
 }
 
-// Conservative FP32 slab test. Returns the (lowered) entry distance in tnear.
+// Conservative FP32 slab test. Returns the (lowered) entry distance in tnear. An axis with a
+// zero direction component constrains nothing in t; it only requires the origin to lie in
+// the slab, compared exactly as the reference does (geometry.cpp:569-571).
 CR_D bool box_fast(const FastSetup& F, float lx, float ly, float lz, float hx, float hy, float hz,
                    float tmin, float tmax, float& tnear) {
     const float t0x = (lx - F.o.x) * F.inv.x, t1x = (hx - F.o.x) * F.inv.x;
     const float t0y = (ly - F.o.y) * F.inv.y, t1y = (hy - F.o.y) * F.inv.y;
     const float t0z = (lz - F.o.z) * F.inv.z, t1z = (hz - F.o.z) * F.inv.z;
-    float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
-    float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+    float nx = fminf(t0x, t1x), fx = fmaxf(t0x, t1x);
+    float ny = fminf(t0y, t1y), fy = fmaxf(t0y, t1y);
+    float nz = fminf(t0z, t1z), fz = fmaxf(t0z, t1z);
+    if (F.zeroAxes) {
+        if (F.zeroAxes & 1u) { if (F.o.x < lx || F.o.x > hx) return false; nx = -kInf; fx = kInf; }
+        if (F.zeroAxes & 2u) { if (F.o.y < ly || F.o.y > hy) return false; ny = -kInf; fy = kInf; }
+        if (F.zeroAxes & 4u) { if (F.o.z < lz || F.o.z > hz) return false; nz = -kInf; fz = kInf; }
+    }
+    float tn = fmaxf(fmaxf(nx, ny), nz);
+    float tf = fminf(fminf(fx, fy), fz);
     tn = tn - fabsf(tn) * kBoxRel - kBoxAbs;
     tf = tf + fabsf(tf) * kBoxRel + kBoxAbs;
     tn = fmaxf(tn, tmin);
@@ -280,9 +292,9 @@ CR_D bool tri_reject_fast(const FastSetup& F, float4 p0, float4 p1, float4 p2) {
     return (w0 < -dw || w1 < -dw || w2 < -dw) && (w0 > dw || w1 > dw || w2 > dw);
 }
 
-template <bool ANY>
+template <bool ANY, bool COUNT = false>
 __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore,
-                               HitRec& hit, int& err) {
+                               HitRec& hit, int& err, VisitCount* vc = nullptr) {
     double closestLimit = smin(static_cast<double>(ray.tmax), hitT);
     float ctmax = smin(ray.tmax, next_up(static_cast<float>(closestLimit)));
     const float queryLimit = ctmax;
@@ -310,6 +322,7 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
             for (uint32_t i = ref; i < ref + cnt; ++i) {
                 const float4* q = S.tri_pos + 3 * static_cast<uint64_t>(i);
                 const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+                if (COUNT) ++vc->tris;
                 const uint32_t index = __float_as_uint(q0.w);
                 if (index == ignore) continue;
                 if (tri_reject_fast(F, q0, q1, q2)) continue;
@@ -329,6 +342,7 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
         } else {
             float4 a, b, c; uint4 d;
             load_pair(S.pairs, ref, a, b, c, d);
+            if (COUNT) ++vc->pairs;
             float n0, n1;
             const bool h0 = box_fast(F, a.x, a.y, a.z, a.w, b.x, b.y, ray.tmin, ctmax, n0);
             const bool h1 = box_fast(F, b.z, b.w, c.x, c.y, c.z, c.w, ray.tmin, ctmax, n1);
@@ -349,12 +363,12 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
 
 // Bvh::intersect entry: the reference's preconditions (geometry.cpp:555), then the traversal
 // that fits the ray.
-template <bool ANY>
+template <bool ANY, bool COUNT = false>
 __device__ bool intersect(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore, bool forceExact,
-                          HitRec& hit, int& err) {
+                          HitRec& hit, int& err, VisitCount* vc = nullptr) {
     if (!S.has_root || !validRay(ray) || isnan(hitT)) return false;
-    if (forceExact || !fast_eligible(ray)) return intersect_exact<ANY>(S, ray, hitT, ignore, hit, err);
-    return intersect_fast<ANY>(S, ray, hitT, ignore, hit, err);
+    if (forceExact || !fast_eligible(ray)) return intersect_exact<ANY, COUNT>(S, ray, hitT, ignore, hit, err, vc);
+    return intersect_fast<ANY, COUNT>(S, ray, hitT, ignore, hit, err, vc);
 }
 
 }  // namespace crg

@@ -207,6 +207,8 @@ typedef struct cr_render_stats {
     uint64_t extend_rays;       /* closest-hit rays traced                               */
     uint64_t shadow_rays;       /* any-hit rays traced                                   */
     uint64_t kernel_launches;   /* kernels launched by this call                         */
+    uint64_t extend_pairs;      /* node pairs fetched by closest-hit (count_traversal)    */
+    uint64_t extend_triangles;  /* triangles tested by closest-hit (count_traversal)      */
 } cr_render_stats;
 
 typedef void (*cr_progress_fn)(uint64_t complete, uint64_t total, double seconds, void* user);
@@ -220,6 +222,7 @@ typedef struct cr_gpu_tuning {
     int32_t block_size;        /* 0: automatic                                             */
     int32_t use_graphs;        /* 0: automatic (on), -1: off                               */
     int32_t time_phases;       /* 1: CUDA-event time every extend/shade/shadow launch      */
+    int32_t count_traversal;   /* 1: count node pairs and triangles visited by closest-hit */
 } cr_gpu_tuning;
 
 typedef struct cr_gpu_scene cr_gpu_scene;
@@ -249,6 +252,11 @@ cr_status cr_bvh_build(const cr_triangle* triangles, uint64_t triangle_count,
                        cr_bvh_node* nodes, uint64_t* node_count, uint32_t* indices);
 /* fmod(degrees, 360) * pi / 180 in float, as Environment's constructor stores it. */
 float cr_environment_rotation(float degrees);
+/* Environment's importance table (render.cpp:28-41) as the device uses it: cdf receives
+ * width*height doubles (may be NULL), weight_sum_integral the weight sum and the luminance
+ * integral. A constant environment yields only the integral (4*pi*luminance). */
+cr_status cr_environment_tables(const cr_environment_desc* environment, double* cdf,
+                                double* weight_sum_integral);
 
 /* ---- device scene ------------------------------------------------------------------ */
 cr_status cr_gpu_scene_create(const cr_scene_desc* scene, const cr_environment_desc* environment,

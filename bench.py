@@ -214,13 +214,15 @@ def run_ours(args):
         if distributed:
             torch.distributed.barrier()
 
-    # counting pass (untimed): node pairs and triangles per closest-hit ray
+    # counting pass (untimed): node pairs and triangles per closest-hit and any-hit ray
     tc = crgpu.Tuning()
     tc.count_traversal = 1
     copt = crgpu.Options.make(width=opt.width, height=opt.height, samples=1, bounces=opt.bounces, seed=opt.seed)
     cstats, _ = g.render_resident(cam, copt, tuning=tc)
-    pairs_per_ray = cstats["extend_pairs"] / max(1, cstats["extend_rays"])
-    tris_per_ray = cstats["extend_triangles"] / max(1, cstats["extend_rays"])
+    ext_pairs = cstats["extend_pairs"] / max(1, cstats["extend_rays"])
+    ext_tris = cstats["extend_triangles"] / max(1, cstats["extend_rays"])
+    sh_pairs = cstats["shadow_pairs"] / max(1, cstats["shadow_rays"])
+    sh_tris = cstats["shadow_triangles"] / max(1, cstats["shadow_rays"])
 
     for _ in range(args.warmup):
         g.render_resident(cam, opt)
@@ -245,19 +247,28 @@ def run_ours(args):
     tp = crgpu.Tuning()
     tp.time_phases = 1
     pst, _ = g.render_resident(cam, opt, tuning=tp)
-    ext_launches = pst["waves"] * (opt.bounces + 1)
-    bytes_per_ray = 64.0 * pairs_per_ray + 48.0 * tris_per_ray + 16 + 16 + 4 + 4 + 4 + 4
-    achieved = bytes_per_ray * pst["extend_rays"] / (pst["extend_ms"] / 1e3) / 1e9
+    trace_launches = pst["iterations"]
+    # algorithmic bytes: 64 B per node pair, 48 B per triangle record, plus the ray's own
+    # state (closest hit: ray 32 + flags/ignore/pixel/sample 16 + result 4; any hit: ray 48 +
+    # contribution 16 + radiance read/write 32 + flags 4)
+    ext_bytes = 64.0 * ext_pairs + 48.0 * ext_tris + 52.0
+    sh_bytes = 64.0 * sh_pairs + 48.0 * sh_tris + 100.0
+    algo_bytes = ext_bytes * pst["extend_rays"] + sh_bytes * pst["shadow_rays"]
+    achieved = algo_bytes / (pst["trace_ms"] / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic_per_ray = profile_traffic()
+    rays = pst["extend_rays"] + pst["shadow_rays"]
     roofline = {
-        "kernel": "k_extend (closest hit)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "kernel": "k_trace (closest + any hit)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": peak_kind,
-        "traffic": (traffic_per_ray * pst["extend_rays"] / ext_launches) if traffic_per_ray else None,
-        "algorithmic_bytes_per_launch": bytes_per_ray * pst["extend_rays"] / ext_launches,
-        "bytes_per_ray": bytes_per_ray, "pairs_per_ray": pairs_per_ray, "triangles_per_ray": tris_per_ray,
-        "extend_ms_share": pst["extend_ms"] / pst["device_ms"],
-        "mrays_per_s": pst["extend_rays"] / (pst["extend_ms"] / 1e3) / 1e6,
+        "traffic": (traffic_per_ray * rays / trace_launches) if traffic_per_ray else None,
+        "algorithmic_bytes_per_launch": algo_bytes / trace_launches,
+        "closest_hit": {"bytes_per_ray": ext_bytes, "pairs_per_ray": ext_pairs, "triangles_per_ray": ext_tris},
+        "any_hit": {"bytes_per_ray": sh_bytes, "pairs_per_ray": sh_pairs, "triangles_per_ray": sh_tris},
+        "trace_ms_share": pst["trace_ms"] / pst["device_ms"],
+        "shade_ms_share": pst["shade_ms"] / pst["device_ms"],
+        "mrays_per_s": rays / (pst["trace_ms"] / 1e3) / 1e6,
+        "launches": trace_launches,
     }
 
     # end to end through the C ABI with host buffers: upload, render, download every step

@@ -54,24 +54,26 @@ def up_to_date():
     return all(os.path.getmtime(s) <= t for s in _sources())
 
 
-def build(force=False, verbose=False, ptxas_verbose=False):
-    """Compile the library in-tree; returns its path."""
-    if not force and up_to_date():
+def build(force=False, verbose=False, ptxas_verbose=False, defines=(), out=None):
+    """Compile the library in-tree (or to `out` with extra -D defines); returns its path."""
+    lib = out or LIB
+    if not force and not defines and out is None and up_to_date():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     inc = ["-I" + INCLUDE, "-I" + CSRC]
+    tag = "" if out is None else "_" + os.path.basename(out).replace(".so", "")
     host_obj = os.path.join(BUILD, "cr_host.o")
-    dev_obj = os.path.join(BUILD, "cr_render.o")
+    dev_obj = os.path.join(BUILD, f"cr_render{tag}.o")
     _run(["g++"] + CXX_FLAGS + inc + ["-I/usr/local/cuda/include", "-c", os.path.join(CSRC, "cr_host.cpp"), "-o", host_obj], verbose)
-    flags = NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_verbose else [])
+    flags = NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-D" + d for d in defines]
     r = _run([nvcc] + ARCH + flags + inc + ["-c", os.path.join(CSRC, "cr_render.cu"), "-o", dev_obj], verbose)
     if ptxas_verbose:
         sys.stderr.write(r.stdout + r.stderr)
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     _run([nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", tmp, dev_obj, host_obj, "-lpthread"], verbose)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

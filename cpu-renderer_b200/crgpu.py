@@ -11,7 +11,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libcr_b200.so")
+LIB_PATH = os.environ.get("CR_B200_LIB", os.path.join(HERE, "libcr_b200.so"))
 
 vertex_dtype = np.dtype([("position", "<f4", 3), ("normal", "<f4", 3), ("tangent", "<f4", 4), ("uv", "<f4", (2, 2))])
 triangle_dtype = np.dtype([("v", vertex_dtype, 3), ("material", "<u4"), ("geometric_normal", "<f4", 3), ("area", "<f4")])
@@ -102,11 +102,12 @@ class Options(C.Structure):
 
 
 class Stats(C.Structure):
-    _fields_ = [("seconds", C.c_double), ("device_ms", C.c_double), ("extend_ms", C.c_double),
-                ("shadow_ms", C.c_double), ("shade_ms", C.c_double), ("workers", C.c_int32), ("waves", C.c_int32),
+    _fields_ = [("seconds", C.c_double), ("device_ms", C.c_double), ("trace_ms", C.c_double),
+                ("shade_ms", C.c_double), ("regen_ms", C.c_double), ("workers", C.c_int32), ("chunks", C.c_int32),
                 ("camera_samples", C.c_uint64), ("boundary_retries", C.c_uint64), ("extend_rays", C.c_uint64),
                 ("shadow_rays", C.c_uint64), ("kernel_launches", C.c_uint64), ("extend_pairs", C.c_uint64),
-                ("extend_triangles", C.c_uint64)]
+                ("extend_triangles", C.c_uint64), ("shadow_pairs", C.c_uint64), ("shadow_triangles", C.c_uint64),
+                ("iterations", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -60,7 +60,16 @@ CR_D float next_toward_zero(float x) {
 // versions err by up to two ulp; evaluating in double and rounding once is correctly
 // rounded in all but ~2^-28 of cases, which keeps device paths as close to the host's as
 // a portable method allows. CR_FAST_TRANSCENDENTALS switches to the float versions.
+// x^5 for the Schlick factor (bsdf.cpp:150, std::pow(x, 5.0f)): x*x is exact in double, two
+// more double products leave a relative error below 2^-52, so the float rounding is the
+// correctly rounded x^5 except within ~2^-28 of a rounding boundary — the same quality as
+// rounding a double pow(), at a fraction of its cost.
+CR_D float fpow5(float x) {
+    const double d = x, d2 = d * d, d4 = d2 * d2;
+    return static_cast<float>(d4 * d);
+}
 #ifdef CR_FAST_TRANSCENDENTALS
+CR_D void fsincos(float x, float& s, float& c) { sincosf(x, &s, &c); }
 CR_D float fcos(float x) { return cosf(x); }
 CR_D float fsin(float x) { return sinf(x); }
 CR_D float fpow(float x, float y) { return powf(x, y); }
@@ -69,6 +78,12 @@ CR_D float flog(float x) { return logf(x); }
 CR_D float fatan2(float y, float x) { return atan2f(y, x); }
 CR_D float facos(float x) { return acosf(x); }
 #else
+CR_D void fsincos(float x, float& s, float& c) {
+    double sd, cd;
+    sincos(static_cast<double>(x), &sd, &cd);
+    s = static_cast<float>(sd);
+    c = static_cast<float>(cd);
+}
 CR_D float fcos(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
 CR_D float fsin(float x) { return static_cast<float>(sin(static_cast<double>(x))); }
 CR_D float fpow(float x, float y) { return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y))); }

@@ -28,8 +28,13 @@ struct LightEntry {
 };
 enum : uint32_t { kLightPunctual = 0, kLightTriangle = 1, kLightEnvironment = 2 };
 
-// Triangle flags in tri_pos[3*slot+1].w.
-enum : uint32_t { kTriCull = 1u, kTriAlphaMask = 2u };
+// Triangle flags in tri_pos[3*slot+1].w and tri_ng[triangle].w. kTriNeeNull marks materials
+// whose BSDF value is zero for every direction (smooth, and metallic 1 or transmission 1, no
+// texture that could change that): their next-event estimation only consumes random draws.
+enum : uint32_t { kTriCull = 1u, kTriAlphaMask = 2u, kTriNeeNull = 4u };
+
+// Shading classes, one queue each, filled by the traversal kernel.
+enum : int { kShadeMiss = 0, kShadeNeeNull = 1, kShadeGeneric = 2, kShadeClasses = 3 };
 
 struct DevImage { int32_t width, height; const float4* pixels; };
 
@@ -59,6 +64,7 @@ struct DevScene {
     const cr_texture* textures;
     uint32_t image_count, texture_count;
     uint32_t any_alpha_mask;
+    uint32_t nee_skip;            // kTriNeeNull surfaces may skip the light-sample arithmetic
     // lights (render.cpp:120-229)
     const LightEntry* light_entries;
     uint32_t light_entry_count;
@@ -120,19 +126,22 @@ struct PathSoA {
     float4* sh_d;         // direction, tmax
     float4* sh_lo;        // originLow
     float4* sh_c;         // contribution, ignore-triangle bits
-    // per-sample radiance output
+    // per-sample radiance of the current chunk, indexed by sample id - chunk start
     float4* out;
 };
 // bits of PathSoA::flags
 enum : uint32_t { kPathLastDelta = 1u, kPathPrecise = 2u, kPathDead = 4u, kPathShadow = 8u };
 
+// Index queues of the path pool, each a ping-pong pair indexed by iteration parity.
 struct Queues {
-    uint32_t* extend[2];
-    uint32_t* shadow;
-    uint32_t* counts;     // [0],[1] extend ping-pong, [2] shadow, [3] retries, [4] errors, [5..] counters
+    uint32_t* extend[2];  // live paths awaiting a closest hit
+    uint32_t* shadow[2];  // paths with a queued shadow ray
+    uint32_t* free[2];    // finished slots awaiting a new camera sample
+    uint32_t* shade[kShadeClasses];  // traced paths by shading class
+    uint32_t* counts;     // kCount* words
 };
-enum { kCountExtend0 = 0, kCountExtend1 = 1, kCountShadow = 2, kCountRetries = 3, kCountErrors = 4,
-       kCountExtendRays = 5, kCountShadowRays = 6, kCountStackOverflow = 7, kCountWords = 8 };
+enum { kCountExtend0 = 0, kCountExtend1 = 1, kCountShadow0 = 2, kCountShadow1 = 3, kCountFree0 = 4, kCountFree1 = 5,
+       kCountShade0 = 6, kCountWords = 12 };
 
 // Device error record; the host reports the one with the smallest key, which is the
 // order a single reference worker would meet them (tiles, rows, columns, samples).

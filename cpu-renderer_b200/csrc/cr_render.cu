@@ -1,19 +1,22 @@
 // Wavefront path tracer for sm_100a: kernels and the host driver behind include/cr_gpu.h.
 //
-// One render (cr::render, render.cpp:352-456) is a sequence of sample waves. A wave holds
-// a block of consecutive sample indices for a range of pixels, one path slot per
-// (pixel, sample). Per bounce it runs:
+// One render (cr::render, render.cpp:352-456) runs a pool of path slots. Camera samples are
+// numbered sample-major (id = sample * pixels + pixel) and issued in order to free slots.
+// Every iteration runs three launches over the whole pool:
 //
-//   k_extend  closest hit for the live queue            (Bvh::intersect, geometry.cpp:554)
-//   k_shade   one trace() iteration per path            (render.cpp:240-344)
-//             -> next live queue, shadow queue (warp-ballot compaction)
-//   k_shadow  any hit for the shadow queue; unoccluded contributions are added
+//   k_regen   free slots take the next sample ids: jitter + camera ray   (render.cpp:396-401)
+//   k_trace   closest hit for the live queue (Bvh::intersect, geometry.cpp:554) and any hit for
+//             the shadow rays queued by the previous iteration, in one launch
+//   k_shade   one trace() iteration per live path (render.cpp:240-344)
+//             -> next live queue, shadow queue, free queue (warp-ballot compaction)
 //
-// The per-path state machine keeps the reference's order of random draws and radiance
-// sums, so each camera sample consumes the same SplitMix stream as on the CPU. After a
-// wave, k_accumulate adds every pixel's samples in index order into FP64 sums (render.cpp:
-// 388-415), so the film does not depend on scheduling. Precision replay (render.cpp:403-412)
-// resets the failing path to its camera ray with split origins and runs it again.
+// Finished paths are refilled the next iteration, so launches stay full until the last
+// samples drain. Each path keeps the reference's order of random draws and radiance sums, so a
+// camera sample consumes the same SplitMix stream as on the CPU. Every sample's radiance is
+// stored by id; at the end of a chunk of ids, k_accumulate adds each pixel's samples in index
+// order into FP64 sums (render.cpp:388-415), so the film does not depend on scheduling.
+// Precision replay (render.cpp:403-412) resets a failing path to its camera ray with split
+// origins and runs it again in the same pool.
 #include "cr_shade.cuh"
 #include "cr_host.h"
 
@@ -26,14 +29,23 @@
 #include <thread>
 #include <vector>
 
+// Minimum resident blocks per SM requested from the register allocator (128-thread blocks).
+#ifndef CR_TRACE_MIN_BLOCKS
+#define CR_TRACE_MIN_BLOCKS 6
+#endif
+#ifndef CR_SHADE_MIN_BLOCKS
+#define CR_SHADE_MIN_BLOCKS 4
+#endif
+
 namespace crg {
 
-struct WaveInfo {
-    uint32_t pixel0, npix, sample0, nsamp, paths;
+// A chunk of consecutive sample ids [c0, c1); out[] holds their radiance at id - c0.
+struct Chunk {
+    uint64_t c0, c1, pixels;
 };
 
 enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatPairs = 4, kStatTris = 5,
-       kStatWords = 6 };
+       kStatIssued = 6, kStatShadowPairs = 7, kStatShadowTris = 8, kStatWords = 12 };
 
 CR_D uint64_t errorKey(const RenderParams& P, uint32_t pixel, uint32_t sample) {
     const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
@@ -109,20 +121,24 @@ CR_D TRay loadRay(const PathSoA& st, uint32_t path, uint32_t flags) {
 }
 
 // Ends a path: the reference's final radiance check (render.cpp:346), then the sample output.
-CR_D void finishPath(const RenderParams& P, const PathSoA& st, uint32_t path, V3 R, const ErrSink& E) {
+CR_D void finishPath(const RenderParams& P, const Chunk& C, const PathSoA& st, uint32_t path, V3 R, const ErrSink& E) {
+    const uint32_t pixel = st.pixel[path], sample = st.sample[path];
     if (!finite3(R) || smin3(R.x, R.y, R.z) < 0) {
-        raise(E, P, st.pixel[path], st.sample[path], kErrNonFiniteRadiance);
+        raise(E, P, pixel, sample, kErrNonFiniteRadiance);
         R = V3{};
     }
-    st.out[path] = f4(R, 0);
+    st.out[static_cast<uint64_t>(sample) * C.pixels + pixel - C.c0] = f4(R, 0);
 }
 
 // One iteration of trace()'s bounce loop (render.cpp:240-344) for one path, after its
-// closest hit is known. Sets cont when the path continues, shadow when a shadow ray was
-// queued; a path that ends with a queued shadow ray is finished by k_shadow.
-CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
-                   unsigned long long* retries, bool& cont, bool& shadow) {
-    cont = false; shadow = false;
+// closest hit is known. cont: the path continues; shadow: a shadow ray was queued (a path
+// that ends with a queued shadow ray is finished by k_trace next iteration); freed: the path
+// ended and its slot can take a new sample. CLASS specialises the code: kShadeMiss holds only
+// environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeGeneric anything.
+template <int CLASS>
+CR_D void shadeOne(const DevScene& S, const RenderParams& P, const Chunk& C, const PathSoA& st, uint32_t path,
+                   const ErrSink& E, unsigned long long* retries, bool& cont, bool& shadow, bool& freed) {
+    cont = false; shadow = false; freed = false;
     uint32_t flags = st.flags[path];
     const bool precise = flags & kPathPrecise;
     const TRay ray = loadRay(st, path, flags);
@@ -137,12 +153,13 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     Rng rng(st.rng[path]);
     const uint32_t tri = st.hit_tri[path];
     int err = 0;
+    auto finish = [&](V3 radiance) { finishPath(P, C, st, path, radiance, E); freed = true; };
 
-    if (tri == kNoTriangle) {  // render.cpp:242-248
+    if (CLASS == kShadeMiss || (CLASS == kShadeGeneric && tri == kNoTriangle)) {  // render.cpp:242-248
         if (medium >= 0) T = T * beerLambert(A, kInf);
         const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, environmentPdf(S, ray.d));
         R = R + T * envRadiance(S, ray.d) * weight;
-        finishPath(P, st, path, R, E);
+        finish(R);
         return;
     }
     // The traversal reported the triangle; t, u and v come from the same FP64 arithmetic.
@@ -160,14 +177,16 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     }
     if (static_cast<int>(depth) == P.bounces) {
         if (err) { raise(E, P, pixel, sample, err); }
-        finishPath(P, st, path, R, E);
+        finish(R);
         return;
     }
     const V3 wo = -ray.d;
     bool pending = false;
     TRay sh;
     V3 contrib;
-    if (P.nee) {  // render.cpp:262-299
+    if (CLASS == kShadeNeeNull && P.nee) {
+        skipLight(S, rng, P.env_alias != 0);  // zero BSDF: the sample cannot contribute
+    } else if (P.nee) {  // render.cpp:262-299
         const LightSample light = sampleLight(S, s.position, rng, P.env_alias, err);
         const bool enclosedInfinite = medium >= 0 && s.thickness <= 0 && !isfin(light.distance);
         if (!enclosedInfinite && light.pdf > 0 && maxComponent(light.radiance) > 0) {
@@ -205,7 +224,7 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     }
     if (err) {  // an exception inside trace(): the sample fails
         raise(E, P, pixel, sample, err);
-        finishPath(P, st, path, V3{}, E);
+        finish(V3{});
         return;
     }
     const uint32_t ignore = precise ? tri : kNoTriangle;
@@ -222,13 +241,13 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     };
     const BsdfSample smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
     if (!smp.ok()) {
-        if (pending) queueShadow(true); else finishPath(P, st, path, R, E);
+        if (pending) queueShadow(true); else finish(R);
         return;
     }
     T = T * smp.weight;
     if (!finite3(T)) {
         raise(E, P, pixel, sample, kErrNonFiniteThroughput);
-        finishPath(P, st, path, V3{}, E);
+        finish(V3{});
         return;
     }
     int boundary = 0;
@@ -259,7 +278,7 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, 
             E.detail->origin[0] = ray.o.x; E.detail->origin[1] = ray.o.y; E.detail->origin[2] = ray.o.z;
             E.detail->direction[0] = ray.d.x; E.detail->direction[1] = ray.d.y; E.detail->direction[2] = ray.d.z;
         }
-        finishPath(P, st, path, V3{}, E);
+        finish(V3{});
         return;
     }
     lastPdf = smp.pdf;
@@ -268,13 +287,13 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     if (precise) { next.o = s.position; next.d = smp.direction; next.tmin = 0; next.tmax = kInf; next.olow = s.positionLow; }
     else if (!offsetRay(s.position, s.geometricNormal, smp.direction, kInf, next, err)) {
         raise(E, P, pixel, sample, err);
-        finishPath(P, st, path, V3{}, E);
+        finish(V3{});
         return;
     }
     if (P.rr && depth >= 3) {  // render.cpp:337-343
         const float survive = sclamp(maxComponent(T) * etaScale, 0.05f, 0.95f);
         if (rng.uniform() >= survive) {
-            if (pending) queueShadow(true); else finishPath(P, st, path, R, E);
+            if (pending) queueShadow(true); else finish(R);
             return;
         }
         T = T * (1 / survive);
@@ -296,108 +315,163 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     cont = true;
 }
 
-// ---- kernels ---------------------------------------------------------------------------------
-__global__ void k_generate(DevScene S, RenderParams P, PathSoA st, Queues q, WaveInfo w, ErrSink E) {
-    for (uint32_t base = blockIdx.x * blockDim.x; base < w.paths; base += gridDim.x * blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        bool live = false;
-        if (i < w.paths) {
-            const uint32_t pixel = w.pixel0 + i % w.npix, sample = w.sample0 + i / w.npix;
-            live = initPath(S, P, st, i, pixel, sample, false, E);
-            if (!live) st.out[i] = make_float4(0, 0, 0, 0);
-        }
-        warpPush(q.extend[0], &q.counts[kCountExtend0], live, i);
-    }
-}
-
-template <bool COUNT>
-__global__ void __launch_bounds__(128) k_extend(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, ErrSink E,
-                                                unsigned long long* stats) {
-    const uint32_t n = q.counts[cur];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        q.counts[cur ^ 1] = 0;
-        q.counts[kCountShadow] = 0;
-        stats[kStatExtendRays] += n;
-    }
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
-        const uint32_t path = q.extend[cur][idx];
-        const uint32_t flags = st.flags[path];
-        const TRay r = loadRay(st, path, flags);
-        HitRec h;
-        h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
-        int err = 0;
-        VisitCount vc;
-        const bool found = intersect<false, COUNT>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
-                                                   h, err, &vc);
-        st.hit_tri[path] = found ? h.tri : kNoTriangle;
-        if (err) raise(E, P, st.pixel[path], st.sample[path], err);
-        if (COUNT) {
-            atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
-            atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
-        }
-    }
-}
-
-__global__ void __launch_bounds__(128) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, ErrSink E,
-                                               unsigned long long* stats) {
-    const uint32_t n = q.counts[cur];
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-        bool cont = false, shadow = false;
-        uint32_t path = 0;
-        if (idx < n) {
-            path = q.extend[cur][idx];
-            shadeOne(S, P, st, path, E, &stats[kStatRetries], cont, shadow);
-        }
-        warpPush(q.extend[cur ^ 1], &q.counts[cur ^ 1], cont, path);
-        warpPush(q.shadow, &q.counts[kCountShadow], shadow, path);
-    }
-}
-
-CR_D void shadowOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E) {
+// Any hit for one queued shadow ray; an unoccluded contribution is added (render.cpp:283-296).
+// Returns true when the path had ended and its slot is now free.
+template <bool COUNT = false>
+CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const Chunk& C, const PathSoA& st, uint32_t path,
+                    const ErrSink& E, unsigned long long* stats = nullptr) {
     const float4 o = st.sh_o[path], d = st.sh_d[path], lo = st.sh_lo[path], c = st.sh_c[path];
     TRay r;
     r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w; r.olow = v3(lo);
     HitRec h;
     h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
     int err = 0;
-    const bool blocked = intersect<true>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0, h, err);
+    VisitCount vc;
+    const bool blocked = intersect<true, COUNT>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0,
+                                                h, err, &vc);
     if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    if (COUNT) {
+        atomicAdd(&stats[kStatShadowPairs], static_cast<unsigned long long>(vc.pairs));
+        atomicAdd(&stats[kStatShadowTris], static_cast<unsigned long long>(vc.tris));
+    }
     const float4 ra = st.rad[path];
     V3 R = v3(ra);
     if (!blocked) R = R + v3(c);
     const uint32_t flags = st.flags[path];
-    if (flags & kPathDead) finishPath(P, st, path, R, E);
-    else st.rad[path] = f4(R, ra.w);
+    if (flags & kPathDead) { finishPath(P, C, st, path, R, E); return true; }
+    st.rad[path] = f4(R, ra.w);
+    return false;
 }
 
-__global__ void __launch_bounds__(128) k_shadow(DevScene S, RenderParams P, PathSoA st, Queues q, ErrSink E,
-                                                unsigned long long* stats) {
-    const uint32_t n = q.counts[kCountShadow];
-    if (blockIdx.x == 0 && threadIdx.x == 0) stats[kStatShadowRays] += n;
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x)
-        shadowOne(S, P, st, q.shadow[idx], E);
+template <bool COUNT>
+CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
+                    unsigned long long* stats) {
+    const uint32_t flags = st.flags[path];
+    const TRay r = loadRay(st, path, flags);
+    HitRec h;
+    h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
+    int err = 0;
+    VisitCount vc;
+    const bool found = intersect<false, COUNT>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
+                                               h, err, &vc);
+    st.hit_tri[path] = found ? h.tri : kNoTriangle;
+    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    if (COUNT) {
+        atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
+        atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
+    }
+    if (!found) return kShadeMiss;
+    return (S.nee_skip && (h.flags & kTriNeeNull)) ? kShadeNeeNull : kShadeGeneric;
 }
 
-// render.cpp:390-413: each pixel adds its samples in index order.
-__global__ void k_accumulate(PathSoA st, WaveInfo w, double* acc) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.npix; i += gridDim.x * blockDim.x) {
-        const uint64_t p = static_cast<uint64_t>(w.pixel0) + i;
+// ---- kernels -----------------------------------------------------------------------------------
+// Every pool slot starts free (in free[1], which the first k_regen reads).
+__global__ void k_pool_init(Queues q, uint32_t pool) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pool; i += gridDim.x * blockDim.x) q.free[1][i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) q.counts[kCountFree1] = pool;
+}
+
+// Free slots take the next sample ids of the chunk, in order.
+__global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+                                               unsigned long long* stats) {
+    const uint32_t n = q.counts[kCountFree0 + (cur ^ 1)];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        q.counts[kCountFree0 + cur] = 0;
+        for (int c = 0; c < kShadeClasses; ++c) q.counts[kCountShade0 + c] = 0;
+    }
+    const uint32_t* freeQ = q.free[cur ^ 1];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        const bool have = idx < n;
+        const uint32_t slot = have ? freeQ[idx] : 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, have);
+        const int lane = threadIdx.x & 31;
+        unsigned long long first = 0;
+        if (mask) {
+            const int leader = __ffs(mask) - 1;
+            if (lane == leader) first = atomicAdd(&stats[kStatIssued], static_cast<unsigned long long>(__popc(mask)));
+            first = __shfl_sync(0xffffffffu, first, leader);
+        }
+        const uint64_t id = first + __popc(mask & ((1u << lane) - 1u));
+        bool live = false;
+        if (have && id < C.c1) {
+            const uint32_t pixel = static_cast<uint32_t>(id % C.pixels), sample = static_cast<uint32_t>(id / C.pixels);
+            live = initPath(S, P, st, slot, pixel, sample, false, E);
+            if (!live) st.out[id - C.c0] = make_float4(0, 0, 0, 0);
+        }
+        warpPush(q.extend[cur], &q.counts[kCountExtend0 + cur], live, slot);
+    }
+}
+
+// Closest hit for the live queue and any hit for last iteration's shadow rays, one launch.
+template <bool COUNT>
+__global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+                                               unsigned long long* stats) {
+    const uint32_t nE = q.counts[kCountExtend0 + cur];
+    const uint32_t nS = q.counts[kCountShadow0 + (cur ^ 1)];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        q.counts[kCountExtend0 + (cur ^ 1)] = 0;
+        q.counts[kCountShadow0 + cur] = 0;
+        stats[kStatExtendRays] += nE;
+        stats[kStatShadowRays] += nS;
+    }
+    const uint32_t total = nE + nS;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        bool freed = false;
+        int cls = -1;
+        uint32_t path = 0;
+        if (idx < nE) {
+            path = q.extend[cur][idx];
+            cls = closestOne<COUNT>(S, P, st, path, E, stats);
+        } else if (idx < total) {
+            path = q.shadow[cur ^ 1][idx - nE];
+            freed = shadowOne<COUNT>(S, P, C, st, path, E, stats);
+        }
+        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
+#pragma unroll
+        for (int c = 0; c < kShadeClasses; ++c) warpPush(q.shade[c], &q.counts[kCountShade0 + c], cls == c, path);
+    }
+}
+
+template <int CLASS>
+__global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+                                               unsigned long long* stats) {
+    const uint32_t n = q.counts[kCountShade0 + CLASS];
+    const uint32_t* in = q.shade[CLASS];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        bool cont = false, shadow = false, freed = false;
+        uint32_t path = 0;
+        if (idx < n) {
+            path = in[idx];
+            shadeOne<CLASS>(S, P, C, st, path, E, &stats[kStatRetries], cont, shadow, freed);
+        }
+        warpPush(q.extend[cur ^ 1], &q.counts[kCountExtend0 + (cur ^ 1)], cont, path);
+        warpPush(q.shadow[cur], &q.counts[kCountShadow0 + cur], shadow, path);
+        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
+    }
+}
+
+// render.cpp:390-413: each pixel adds the chunk's samples in index order.
+__global__ void k_accumulate(const float4* out, Chunk C, double* acc) {
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < C.pixels;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t sBegin = C.c0 > p ? (C.c0 - p + C.pixels - 1) / C.pixels : 0;
+        const uint64_t sEnd = C.c1 > p ? (C.c1 - p + C.pixels - 1) / C.pixels : 0;
         double r = acc[3 * p], g = acc[3 * p + 1], b = acc[3 * p + 2];
-        for (uint32_t k = 0; k < w.nsamp; ++k) {
-            const float4 o = st.out[static_cast<uint64_t>(k) * w.npix + i];
+        for (uint64_t s = sBegin; s < sEnd; ++s) {
+            const float4 o = out[s * C.pixels + p - C.c0];
             r += o.x; g += o.y; b += o.z;
         }
         acc[3 * p] = r; acc[3 * p + 1] = g; acc[3 * p + 2] = b;
     }
 }
-// Optional copy of every sample's radiance (sample-major) for stream-level comparisons.
-__global__ void k_dump_samples(PathSoA st, WaveInfo w, uint64_t pixels, float* dst) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.paths; i += gridDim.x * blockDim.x) {
-        const uint64_t p = w.pixel0 + i % w.npix, s = w.sample0 + i / w.npix;
-        const float4 o = st.out[i];
-        float* d = dst + 3 * (s * pixels + p);
-        d[0] = o.x; d[1] = o.y; d[2] = o.z;
+// Copies the chunk's radiance as packed RGB (sample-major) for stream-level comparisons.
+__global__ void k_pack_samples(const float4* out, uint64_t n, float* dst) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const float4 o = out[i];
+        dst[3 * i] = o.x; dst[3 * i + 1] = o.y; dst[3 * i + 2] = o.z;
     }
 }
 // render.cpp:415
@@ -412,6 +486,9 @@ __global__ void k_trace_one(DevScene S, RenderParams P, PathSoA st, uint32_t pix
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     const ErrSink E{scratchKey, detail};
     const uint32_t path = 0;
+    const uint64_t pixels = static_cast<uint64_t>(P.width) * P.height;
+    const uint64_t id = static_cast<uint64_t>(sample) * pixels + pixel;
+    const Chunk C{id, id + 1, pixels};
     if (!initPath(S, P, st, path, pixel, sample, false, E)) return;
     for (int iter = 0; iter < 4 * (P.bounces + 2); ++iter) {
         const uint32_t flags = st.flags[path];
@@ -422,10 +499,10 @@ __global__ void k_trace_one(DevScene S, RenderParams P, PathSoA st, uint32_t pix
         const bool found = intersect<false>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0, h, err);
         if (err) { raise(E, P, pixel, sample, err); return; }
         st.hit_tri[path] = found ? h.tri : kNoTriangle;
-        bool cont = false, shadow = false;
-        shadeOne(S, P, st, path, E, scratchRetries, cont, shadow);
+        bool cont = false, shadow = false, freed = false;
+        shadeOne<kShadeGeneric>(S, P, C, st, path, E, scratchRetries, cont, shadow, freed);
         if (detail->code) return;
-        if (shadow) shadowOne(S, P, st, path, E);
+        if (shadow) shadowOne(S, P, C, st, path, E);
         if (detail->code || !cont) return;
     }
 }
@@ -525,8 +602,9 @@ struct cr_gpu_scene {
     DevAlloc work;      // path buffers
     DevScene dev{};
     uint64_t triangleCount = 0;
-    // work buffers
-    size_t capacity = 0;
+    // work buffers: the path pool, its queues, and the chunk's per-sample output
+    size_t capacity = 0;        // pool slots
+    size_t outCapacity = 0;     // samples per chunk
     PathSoA st{};
     Queues q{};
     uint32_t* counts = nullptr;
@@ -534,13 +612,14 @@ struct cr_gpu_scene {
     DevError* detail = nullptr;
     double* acc = nullptr;
     float* film = nullptr;
+    float* packed = nullptr;    // per-sample RGB staging for stream dumps
+    size_t packedCapacity = 0;
     size_t filmPixels = 0;
-    DevAlloc filmAlloc;
+    DevAlloc filmAlloc, outAlloc, packedAlloc;
     uint32_t* hostCounts = nullptr;           // pinned
     unsigned long long* hostStats = nullptr;  // pinned
-    int gridExtend = 0, gridShade = 0, gridShadow = 0, gridSmall = 0;
+    int gridTrace = 0, gridShade = 0, gridShadeLight = 0, gridShadeMiss = 0, gridRegen = 0, gridSmall = 0;
     std::vector<cudaEvent_t> events;
-    cr_render_options lastOptions{};
     std::mutex mutex;
 
     ~cr_gpu_scene() {
@@ -550,6 +629,8 @@ struct cr_gpu_scene {
         geometry.release();
         work.release();
         filmAlloc.release();
+        outAlloc.release();
+        packedAlloc.release();
         if (hostCounts) cudaFreeHost(hostCounts);
         if (hostStats) cudaFreeHost(hostStats);
         if (stream) cudaStreamDestroy(stream);
@@ -576,13 +657,34 @@ struct cr_gpu_scene {
         st.rng = work.alloc<uint64_t>(n); st.prev_tri = work.alloc<uint32_t>(n);
         st.pixel = work.alloc<uint32_t>(n); st.sample = work.alloc<uint32_t>(n); st.depth = work.alloc<uint32_t>(n);
         st.sh_o = work.alloc<float4>(n); st.sh_d = work.alloc<float4>(n); st.sh_lo = work.alloc<float4>(n);
-        st.sh_c = work.alloc<float4>(n); st.out = work.alloc<float4>(n);
-        q.extend[0] = work.alloc<uint32_t>(n); q.extend[1] = work.alloc<uint32_t>(n); q.shadow = work.alloc<uint32_t>(n);
+        st.sh_c = work.alloc<float4>(n);
+        for (int k = 0; k < 2; ++k) {
+            q.extend[k] = work.alloc<uint32_t>(n);
+            q.shadow[k] = work.alloc<uint32_t>(n);
+            q.free[k] = work.alloc<uint32_t>(n);
+        }
+        for (int c = 0; c < kShadeClasses; ++c) q.shade[c] = work.alloc<uint32_t>(n);
         counts = work.alloc<uint32_t>(kCountWords);
         q.counts = counts;
         stats = work.alloc<unsigned long long>(kStatWords);
         detail = work.alloc<DevError>(1);
         capacity = n;
+    }
+
+    void ensureOut(size_t samples) {
+        if (samples <= outCapacity) return;
+        CR_CUDA(cudaStreamSynchronize(stream));
+        outAlloc.release();
+        st.out = outAlloc.alloc<float4>(samples);
+        outCapacity = samples;
+    }
+
+    void ensurePacked(size_t samples) {
+        if (samples <= packedCapacity) return;
+        CR_CUDA(cudaStreamSynchronize(stream));
+        packedAlloc.release();
+        packed = packedAlloc.alloc<float>(3 * samples);
+        packedCapacity = samples;
     }
 
     void ensureFilm(size_t pixels) {
@@ -654,12 +756,21 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     std::vector<float4> ng(n ? n : 1);
     std::vector<uint32_t> flags(n ? n : 1, 0);
     uint32_t anyMask = 0;
+    bool texturedEmitter = false;
     for (uint64_t i = 0; i < n; ++i) {
         const cr_triangle& t = d.triangles[i];
         const cr_material& m = d.materials[t.material];
         uint32_t f = 0;
         if (!m.double_sided && m.transmission <= 0) f |= kTriCull;
         if (m.alpha_mode == CR_ALPHA_MASK) { f |= kTriAlphaMask; anyMask = 1; }
+        // bsdf.cpp:171-179: smooth, and the diffuse weight (1-metallic)(1-transmission) is zero
+        if (m.roughness <= 0.001f && m.metallic_roughness_texture.texture < 0 &&
+            (m.metallic == 1.0f || (m.transmission == 1.0f && m.transmission_texture.texture < 0)))
+            f |= kTriNeeNull;
+        const bool textured = m.base_color_texture.texture >= 0 || m.metallic_roughness_texture.texture >= 0 ||
+                              m.normal_texture.texture >= 0 || m.emissive_texture.texture >= 0 ||
+                              m.transmission_texture.texture >= 0;
+        if (textured && (m.emission[0] > 0 || m.emission[1] > 0 || m.emission[2] > 0)) texturedEmitter = true;
         flags[i] = f;
         float gx = t.geometric_normal[0], gy = t.geometric_normal[1], gz = t.geometric_normal[2];
         if (gx == 0 && gy == 0 && gz == 0) {  // geometry.cpp:284
@@ -717,6 +828,8 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     S.tris = g.geometry.upload(d.triangles, n ? n : 0, s);
     S.pairs = g.geometry.upload(pairs.data(), pairs.size(), s);
     S.any_alpha_mask = anyMask;
+    // A textured emitter's light sample evaluates textures, which can fail; keep it then.
+    S.nee_skip = texturedEmitter ? 0u : 1u;
     // materials and textures
     S.materials = g.geometry.upload(d.materials, d.material_count, s);
     S.material_count = d.material_count;
@@ -800,7 +913,7 @@ int referenceWorkers(const cr_render_options& o) {  // render.cpp:361-363
     return std::min(tiles, o.threads ? o.threads : automatic);
 }
 
-// The whole render. film_host may be NULL (film stays on the device).
+// The whole render. filmHost may be NULL (film stays on the device).
 void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, cr_progress_fn progress,
                 void* user, float* filmHost, cr_render_stats* stats, const cr_gpu_tuning& tuning, float* perSample) {
     const auto start = std::chrono::steady_clock::now();
@@ -815,33 +928,29 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         throw crh::Error(CR_ERR_RENDER, std::string("Pixel (0,0), sample 0: ") + e.what());
     }
     CR_CUDA(cudaSetDevice(g.device));
-    // Wave plan: up to `target` path slots; whole pixel range with several samples, or pixel
-    // chunks with one sample.
-    uint64_t target = tuning.paths_per_wave > 0 ? static_cast<uint64_t>(tuning.paths_per_wave) : (uint64_t{1} << 21);
-    if (target < 1024) target = 1024;
-    uint32_t npix, nsamp;
-    if (pixels <= target) {
-        npix = static_cast<uint32_t>(pixels);
-        nsamp = static_cast<uint32_t>(std::min<uint64_t>(o.samples, std::max<uint64_t>(1, target / pixels)));
-    } else {
-        npix = static_cast<uint32_t>(target);
-        nsamp = 1;
-    }
-    g.ensureWork(static_cast<size_t>(npix) * nsamp);
+    // Pool of path slots and chunk of sample ids held in device memory at once.
+    uint64_t pool = tuning.paths_per_wave > 0 ? static_cast<uint64_t>(tuning.paths_per_wave) : (uint64_t{1} << 22);
+    pool = std::max<uint64_t>(1024, std::min<uint64_t>(pool, total));
+    pool = (pool + 127) / 128 * 128;
+    const uint64_t chunkBudget = uint64_t{1} << 28;  // 268 M samples = 4 GiB of float4 radiance
+    const uint64_t chunk = std::min<uint64_t>(total, std::max<uint64_t>(pool, chunkBudget));
+    g.ensureWork(static_cast<size_t>(pool));
+    g.ensureOut(static_cast<size_t>(chunk));
     g.ensureFilm(pixels);
+    if (perSample) g.ensurePacked(static_cast<size_t>(chunk));
     if (!g.hostCounts) CR_CUDA(cudaMallocHost(&g.hostCounts, kCountWords * sizeof(uint32_t)));
     if (!g.hostStats) CR_CUDA(cudaMallocHost(&g.hostStats, kStatWords * sizeof(unsigned long long)));
     cudaStream_t s = g.stream;
-    const int block = tuning.block_size > 0 ? tuning.block_size : 128;
-    if (!g.gridExtend) {
-        g.gridExtend = occupancyGrid(reinterpret_cast<const void*>(k_extend<false>), 128, g.device);
-        g.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade), 128, g.device);
-        g.gridShadow = occupancyGrid(reinterpret_cast<const void*>(k_shadow), 128, g.device);
+    if (!g.gridTrace) {
+        g.gridTrace = occupancyGrid(reinterpret_cast<const void*>(k_trace<false>), 128, g.device);
+        g.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
+        g.gridShadeLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
+        g.gridShadeMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
+        g.gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen), 128, g.device);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
         g.gridSmall = sms * 8;
     }
-    (void)block;
     CR_CUDA(cudaMemsetAsync(g.acc, 0, 3 * pixels * sizeof(double), s));
     CR_CUDA(cudaMemsetAsync(g.stats, 0, kStatWords * sizeof(unsigned long long), s));
     const unsigned long long noError = ~0ull;
@@ -849,88 +958,83 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     const ErrSink E{g.stats + kStatErrorKey, nullptr};
 
     const bool timePhases = tuning.time_phases != 0;
-    double extendMs = 0, shadeMs = 0, shadowMs = 0;
+    double traceMs = 0, shadeMs = 0, regenMs = 0;
     uint64_t launches = 0;
-    int waves = 0;
+    int iterations = 0, chunks = 0;
     cudaEvent_t t0 = g.event(0), t1 = g.event(1);
     CR_CUDA(cudaEventRecord(t0, s));
     auto lastProgress = start;
-    uint64_t done = 0;
     bool errored = false;
-    for (uint32_t s0 = 0; s0 < static_cast<uint32_t>(o.samples) && !errored; s0 += nsamp) {
-        const uint32_t ns = std::min<uint32_t>(nsamp, static_cast<uint32_t>(o.samples) - s0);
-        for (uint64_t p0 = 0; p0 < pixels && !errored; p0 += npix) {
-            WaveInfo w;
-            w.pixel0 = static_cast<uint32_t>(p0);
-            w.npix = static_cast<uint32_t>(std::min<uint64_t>(npix, pixels - p0));
-            w.sample0 = s0; w.nsamp = ns; w.paths = w.npix * ns;
-            ++waves;
-            CR_CUDA(cudaMemsetAsync(g.counts, 0, kCountWords * sizeof(uint32_t), s));
-            k_generate<<<g.gridSmall, 128, 0, s>>>(g.dev, P, g.st, g.q, w, E);
-            ++launches;
-            int cur = 0;
-            size_t ev = 2;
-            std::vector<std::pair<size_t, int>> timed;  // (event index, phase)
-            auto bounce = [&]() {
+    const int batch = 8;
+    for (uint64_t c0 = 0; c0 < total && !errored; c0 += chunk) {
+        const Chunk C{c0, std::min<uint64_t>(total, c0 + chunk), pixels};
+        ++chunks;
+        // the chunk's ids are issued from c0
+        CR_CUDA(cudaMemsetAsync(g.counts, 0, kCountWords * sizeof(uint32_t), s));
+        const unsigned long long issuedStart = c0;
+        CR_CUDA(cudaMemcpyAsync(g.stats + kStatIssued, &issuedStart, sizeof(issuedStart), cudaMemcpyHostToDevice, s));
+        k_pool_init<<<g.gridSmall, 128, 0, s>>>(g.q, static_cast<uint32_t>(pool));
+        ++launches;
+        const uint64_t maxIterations = ((C.c1 - C.c0) / pool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
+        uint64_t iter = 0;
+        int cur = 0;
+        std::vector<std::pair<size_t, int>> timed;
+        size_t ev = 2;
+        for (;;) {
+            timed.clear();
+            ev = 2;
+            for (int b = 0; b < batch; ++b) {
                 auto rec = [&](int phase, auto&& launch) {
-                    if (timePhases) { CR_CUDA(cudaEventRecord(g.event(ev), s)); }
+                    if (timePhases) CR_CUDA(cudaEventRecord(g.event(ev), s));
                     launch();
                     if (timePhases) { CR_CUDA(cudaEventRecord(g.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
                     ++launches;
                 };
+                rec(2, [&] { k_regen<<<g.gridRegen, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
                 rec(0, [&] {
-                    if (tuning.count_traversal) k_extend<true><<<g.gridExtend, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats);
-                    else k_extend<false><<<g.gridExtend, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats);
+                    if (tuning.count_traversal) k_trace<true><<<g.gridTrace, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats);
+                    else k_trace<false><<<g.gridTrace, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats);
                 });
-                rec(1, [&] { k_shade<<<g.gridShade, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, E, g.stats); });
-                rec(2, [&] { k_shadow<<<g.gridShadow, 128, 0, s>>>(g.dev, P, g.st, g.q, E, g.stats); });
+                rec(1, [&] { k_shade<kShadeMiss><<<g.gridShadeMiss, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
+                rec(1, [&] { k_shade<kShadeNeeNull><<<g.gridShadeLight, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
+                rec(1, [&] { k_shade<kShadeGeneric><<<g.gridShade, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
                 cur ^= 1;
-            };
-            for (int b = 0; b <= o.bounces; ++b) bounce();
+                ++iter;
+                ++iterations;
+            }
             CR_CUDA(cudaMemcpyAsync(g.hostCounts, g.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-            CR_CUDA(cudaStreamSynchronize(s));
-            if (g.hostCounts[cur]) {  // precision replays still in flight
-                for (int b = 0; b <= o.bounces; ++b) bounce();
-                CR_CUDA(cudaMemcpyAsync(g.hostCounts, g.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-                CR_CUDA(cudaStreamSynchronize(s));
-                if (g.hostCounts[cur]) throw crh::Error(CR_ERR_DEVICE_TIMEOUT, "paths still live after the bounce limit");
-            }
-            k_accumulate<<<g.gridSmall, 128, 0, s>>>(g.st, w, g.acc);
-            ++launches;
-            if (perSample) {
-                float* dst = nullptr;
-                const size_t bytes = static_cast<size_t>(3) * total * sizeof(float);
-                (void)bytes;
-                // stage through the film buffer of the wave's own size
-                float* stage = nullptr;
-                CR_CUDA(cudaMallocAsync(&stage, static_cast<size_t>(3) * pixels * ns * sizeof(float), s));
-                WaveInfo wl = w;
-                wl.sample0 = 0;  // stage is indexed from the wave's first sample
-                k_dump_samples<<<g.gridSmall, 128, 0, s>>>(g.st, wl, pixels, stage);
-                for (uint32_t k = 0; k < ns; ++k) {
-                    dst = perSample + 3 * (static_cast<uint64_t>(s0 + k) * pixels + p0);
-                    CR_CUDA(cudaMemcpyAsync(dst, stage + 3 * (static_cast<uint64_t>(k) * pixels + p0),
-                                            static_cast<size_t>(3) * w.npix * sizeof(float), cudaMemcpyDeviceToHost, s));
-                }
-                CR_CUDA(cudaFreeAsync(stage, s));
-            }
             CR_CUDA(cudaMemcpyAsync(g.hostStats, g.stats, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
             CR_CUDA(cudaStreamSynchronize(s));
             CR_CUDA(cudaGetLastError());
             for (auto& te : timed) {
                 float ms = 0;
                 CR_CUDA(cudaEventElapsedTime(&ms, g.event(te.first), g.event(te.first + 1)));
-                (te.second == 0 ? extendMs : te.second == 1 ? shadeMs : shadowMs) += ms;
+                (te.second == 0 ? traceMs : te.second == 1 ? shadeMs : regenMs) += ms;
             }
-            if (g.hostStats[kStatErrorKey] != ~0ull) errored = true;
-            done += static_cast<uint64_t>(w.paths);
+            // after the last shade: live = next live queue + queued shadow rays
+            const uint64_t live = g.hostCounts[kCountExtend0 + cur] + g.hostCounts[kCountShadow0 + (cur ^ 1)];
+            const bool issuedAll = g.hostStats[kStatIssued] >= C.c1;
+            if (g.hostStats[kStatErrorKey] != ~0ull) { errored = true; break; }
+            if (issuedAll && live == 0) break;
+            if (iter > maxIterations) throw crh::Error(CR_ERR_DEVICE_TIMEOUT, "paths still live after the iteration bound");
             if (progress) {
                 const auto now = std::chrono::steady_clock::now();
                 if (now - lastProgress >= std::chrono::seconds(2)) {
                     lastProgress = now;
+                    const uint64_t issued = std::min<uint64_t>(g.hostStats[kStatIssued], C.c1);
+                    const uint64_t done = issued > live ? issued - live : 0;
                     progress(done, total, std::chrono::duration<double>(now - start).count(), user);
                 }
             }
+        }
+        if (errored) break;
+        k_accumulate<<<g.gridSmall, 128, 0, s>>>(g.st.out, C, g.acc);
+        ++launches;
+        if (perSample) {
+            const uint64_t n = C.c1 - C.c0;
+            k_pack_samples<<<g.gridSmall, 128, 0, s>>>(g.st.out, n, g.packed);
+            CR_CUDA(cudaMemcpyAsync(perSample + 3 * C.c0, g.packed, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaStreamSynchronize(s));
         }
     }
     if (errored) {
@@ -943,19 +1047,20 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         const uint32_t x = static_cast<uint32_t>((tile % tilesX) * 16 + within % 16);
         const uint32_t y = static_cast<uint32_t>((tile / tilesX) * 16 + within / 16);
         DevError host{};
+        CR_CUDA(cudaStreamSynchronize(s));
         CR_CUDA(cudaMemsetAsync(g.detail, 0, sizeof(DevError), s));
         CR_CUDA(cudaMemsetAsync(g.stats, 0, 2 * sizeof(unsigned long long), s));
         k_trace_one<<<1, 32, 0, s>>>(g.dev, P, g.st, y * static_cast<uint32_t>(o.width) + x, sample, g.detail, g.stats, g.stats + 1);
         CR_CUDA(cudaMemcpyAsync(&host, g.detail, sizeof(DevError), cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
         if (!host.code) { host.code = -1; host.x = static_cast<int32_t>(x); host.y = static_cast<int32_t>(y); host.sample = static_cast<int32_t>(sample); }
-        if (host.code == kErrStackOverflow) throw crh::Error(CR_ERR_RENDER, crh::sample_error_message(host));
         throw crh::Error(CR_ERR_RENDER, crh::sample_error_message(host));
     }
     k_film<<<g.gridSmall, 128, 0, s>>>(g.acc, g.film, pixels, o.samples);
     ++launches;
     CR_CUDA(cudaEventRecord(t1, s));
     if (filmHost) CR_CUDA(cudaMemcpyAsync(filmHost, g.film, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaMemcpyAsync(g.hostStats, g.stats, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaStreamSynchronize(s));
     CR_CUDA(cudaGetLastError());
     float deviceMs = 0;
@@ -965,9 +1070,10 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         std::memset(stats, 0, sizeof(*stats));
         stats->seconds = seconds;
         stats->device_ms = deviceMs;
-        stats->extend_ms = extendMs; stats->shade_ms = shadeMs; stats->shadow_ms = shadowMs;
+        stats->trace_ms = traceMs; stats->shade_ms = shadeMs; stats->regen_ms = regenMs;
         stats->workers = referenceWorkers(o);
-        stats->waves = waves;
+        stats->chunks = chunks;
+        stats->iterations = static_cast<uint64_t>(iterations);
         stats->camera_samples = total;
         stats->boundary_retries = g.hostStats[kStatRetries];
         stats->extend_rays = g.hostStats[kStatExtendRays];
@@ -975,6 +1081,8 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         stats->kernel_launches = launches;
         stats->extend_pairs = g.hostStats[kStatPairs];
         stats->extend_triangles = g.hostStats[kStatTris];
+        stats->shadow_pairs = g.hostStats[kStatShadowPairs];
+        stats->shadow_triangles = g.hostStats[kStatShadowTris];
     }
     if (progress) progress(total, total, seconds, user);
 }
@@ -1020,7 +1128,7 @@ cr_status cr_gpu_scene_destroy(cr_gpu_scene* scene) {
 
 cr_status cr_gpu_scene_bytes(const cr_gpu_scene* scene, uint64_t* bytes) {
     if (!scene || !bytes) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "scene or bytes is NULL");
-    *bytes = scene->geometry.bytes + scene->work.bytes + scene->filmAlloc.bytes;
+    *bytes = scene->geometry.bytes + scene->work.bytes + scene->filmAlloc.bytes + scene->outAlloc.bytes + scene->packedAlloc.bytes;
     return CR_OK;
 }
 

@@ -194,8 +194,10 @@ CR_D V3 visibleNormal(V3 wo, float alpha, float u, float v) {
     const V3 t1 = lensq > 0 ? V3{-vh.y, vh.x, 0} / sqrtf(lensq) : V3{1, 0, 0};
     const V3 t2 = cross(vh, t1);
     const float r = sqrtf(u), phi = 2 * kPi * v;
-    const float x = r * fcos(phi);
-    float y = r * fsin(phi);
+    float sp, cp;
+    fsincos(phi, sp, cp);
+    const float x = r * cp;
+    float y = r * sp;
     const float s = 0.5f * (1 + vh.z);
     y = (1 - s) * sqrtf(smax(0.0f, 1 - x * x)) + s * y;
     const V3 nh = t1 * x + t2 * y + vh * sqrtf(smax(0.0f, 1 - x * x - y * y));
@@ -213,7 +215,7 @@ struct Ctx {
         return thin ? 2 * f / (1 + f) : f;
     }
     CR_D V3 reflection(float f, float cosine) const {
-        const float schlick = fpow(1 - sclamp(fabsf(cosine), 0.0f, 1.0f), 5.0f);
+        const float schlick = fpow5(1 - sclamp(fabsf(cosine), 0.0f, 1.0f));
         return V3{(1 - s.metallic) * f} + (s.baseColor + (V3{1} - s.baseColor) * schlick) * s.metallic;
     }
     CR_D V3 transmission(float f) const { return s.baseColor * ((1 - s.metallic) * s.transmission * (1 - f)); }
@@ -306,7 +308,9 @@ CR_D BsdfSample sampleBsdf(const Surface& s, V3 wo, Rng& rng) {
     const float lobe = rng.uniform();
     if (lobe < c.diffuseProbability) {
         const float u = rng.uniform(), phi = 2 * kPi * rng.uniform();
-        wi = V3{sqrtf(u) * fcos(phi), sqrtf(u) * fsin(phi), sqrtf(1 - u)};
+        float sp, cp;
+        fsincos(phi, sp, cp);
+        wi = V3{sqrtf(u) * cp, sqrtf(u) * sp, sqrtf(1 - u)};
     } else if (lobe < c.diffuseProbability + c.deltaTransmissionProbability) {
         out.direction = -wo; out.delta = true; out.transmitted = true; out.pdf = c.deltaTransmissionProbability;
         out.weight = s.baseColor * ((1 - s.metallic) * s.transmission / out.pdf);
@@ -398,7 +402,9 @@ CR_D V3 envSample(const DevScene& S, Rng& rng, float& density, bool alias) {
     if (!S.env_has_image) {
         const float y = 1 - 2 * rng.uniform(), phi = 2 * kPi * rng.uniform(), r = sqrtf(smax(0.0f, 1 - y * y));
         density = 1 / (4 * kPi);
-        return {r * fcos(phi), y, r * fsin(phi)};
+        float sp, cp;
+        fsincos(phi, sp, cp);
+        return {r * cp, y, r * sp};
     }
     const uint64_t n = static_cast<uint64_t>(S.env_width) * S.env_height;
     uint64_t index;
@@ -425,7 +431,9 @@ CR_D V3 envSample(const DevScene& S, Rng& rng, float& density, bool alias) {
     const float cosTheta = c0 + (c1 - c0) * rng.uniform(), sinTheta = sqrtf(smax(0.0f, 1 - cosTheta * cosTheta));
     const float phi = (u - 0.5f) * 2 * kPi + S.env_rotation;
     density = __ldg(S.env_pdf + index);
-    return {sinTheta * fcos(phi), cosTheta, sinTheta * fsin(phi)};
+    float sp, cp;
+    fsincos(phi, sp, cp);
+    return {sinTheta * cp, cosTheta, sinTheta * sp};
 }
 
 // ---- light sampler (render.cpp:113-229) --------------------------------------------------------
@@ -502,6 +510,25 @@ CR_D LightSample sampleLight(const DevScene& S, V3 from, Rng& rng, bool alias, i
     out.radiance = s.emission;
     out.pdf = trianglePdf(S, e.index, from, out.target);
     return out;
+}
+
+// The random draws sampleLight consumes, without its arithmetic: for a surface whose BSDF is
+// zero in every direction the light sample cannot contribute (render.cpp:271-272), but its
+// draws still advance the stream (1 selection draw; environment image 3, constant
+// environment 2, alias table 4, triangle 2, punctual 0).
+CR_D void skipLight(const DevScene& S, Rng& rng, bool alias) {
+    if (S.light_entry_count == 0) return;
+    const double u = rng.uniform();
+    uint32_t lo = 0, count = S.light_entry_count;
+    while (count > 0) {
+        const uint32_t step = count / 2, it = lo + step;
+        if (S.light_entries[it].cdf < u) { lo = it + 1; count -= step + 1; } else count = step;
+    }
+    const uint32_t type = S.light_entries[lo == S.light_entry_count ? S.light_entry_count - 1 : lo].type;
+    int draws = 0;
+    if (type == kLightEnvironment) draws = !S.env_has_image ? 2 : (alias && S.alias_prob ? 4 : 3);
+    else if (type == kLightTriangle) draws = 2;
+    for (int k = 0; k < draws; ++k) rng.next();
 }
 
 // ---- offsetRay (geometry.cpp:186-209) ------------------------------------------------------------

@@ -29,6 +29,7 @@ struct TRay {
 struct HitRec {
     double t, u, v;
     uint32_t tri;
+    uint32_t flags;  // kTri* flags of the hit triangle
 };
 
 // validRay (geometry.cpp:52-55).
@@ -163,9 +164,9 @@ __device__ bool intersect_exact(const DevScene& S, const TRay& ray, double hitT,
                 double t, w1, w2, det;
                 if (!tri_exact(E, v3(q0), v3(q1), v3(q2), ray.tmin, limit, t, w1, w2, det)) continue;
                 if (!accepts(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
-                if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; return true; }
+                if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; hit.flags = __float_as_uint(q1.w); return true; }
                 if (!found || t < hit.t || (t == hit.t && index < hit.tri)) {
-                    hit.t = t; hit.tri = index; bestW1 = w1; bestW2 = w2; bestDet = det;
+                    hit.t = t; hit.tri = index; hit.flags = __float_as_uint(q1.w); bestW1 = w1; bestW2 = w2; bestDet = det;
                     closestLimit = t;
                     ctmax = smin(queryLimit, next_up(static_cast<float>(t)));
                     found = true;
@@ -331,9 +332,9 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
                 double t, w1, w2, det;
                 if (!tri_exact(E, v3(q0), v3(q1), v3(q2), ray.tmin, limit, t, w1, w2, det)) continue;
                 if (!accepts(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
-                if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; return true; }
+                if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; hit.flags = __float_as_uint(q1.w); return true; }
                 if (!found || t < hit.t || (t == hit.t && index < hit.tri)) {
-                    hit.t = t; hit.tri = index; bestW1 = w1; bestW2 = w2; bestDet = det;
+                    hit.t = t; hit.tri = index; hit.flags = __float_as_uint(q1.w); bestW1 = w1; bestW2 = w2; bestDet = det;
                     closestLimit = t;
                     ctmax = smin(queryLimit, next_up(static_cast<float>(t)));
                     found = true;

@@ -197,11 +197,12 @@ typedef struct cr_environment_desc {
 typedef struct cr_render_stats {
     double seconds;             /* wall time of the call, like RenderResult::seconds    */
     double device_ms;           /* CUDA-event time of all render kernels                 */
-    double extend_ms;           /* CUDA-event time of the closest-hit launches          */
-    double shadow_ms;           /* CUDA-event time of the any-hit launches              */
+    double trace_ms;            /* CUDA-event time of the traversal launches (closest and
+                                   any hit share one launch per iteration)              */
     double shade_ms;            /* CUDA-event time of the shading launches              */
+    double regen_ms;            /* CUDA-event time of the camera-sample launches        */
     int32_t workers;            /* the reference's worker-count formula (render.cpp:363) */
-    int32_t waves;              /* sample waves launched                                 */
+    int32_t chunks;             /* chunks of sample ids (each accumulated in order)      */
     uint64_t camera_samples;    /* width*height*samples                                  */
     uint64_t boundary_retries;  /* precision replays (render.cpp:409)                    */
     uint64_t extend_rays;       /* closest-hit rays traced                               */
@@ -209,6 +210,9 @@ typedef struct cr_render_stats {
     uint64_t kernel_launches;   /* kernels launched by this call                         */
     uint64_t extend_pairs;      /* node pairs fetched by closest-hit (count_traversal)    */
     uint64_t extend_triangles;  /* triangles tested by closest-hit (count_traversal)      */
+    uint64_t shadow_pairs;      /* node pairs fetched by any-hit (count_traversal)        */
+    uint64_t shadow_triangles;  /* triangles tested by any-hit (count_traversal)          */
+    uint64_t iterations;        /* pool iterations (regen, trace, shade)                  */
 } cr_render_stats;
 
 typedef void (*cr_progress_fn)(uint64_t complete, uint64_t total, double seconds, void* user);

@@ -119,9 +119,9 @@ def test_determinism_across_wave_sizes(crgpu, gpu):
     a, _ = g.render(cam, opt)
     b, _ = g.render(cam, opt)
     t = Tuning()
-    t.paths_per_wave = 5000  # pixel chunks, one sample per wave
+    t.paths_per_wave = 5000  # a small pool: many iterations, samples finish far out of order
     c, st = g.render(cam, opt, tuning=t)
-    assert st["waves"] > 16
+    assert st["iterations"] > 100
     assert a.tobytes() == b.tobytes() == c.tobytes()
 
 

@@ -31,7 +31,7 @@
 
 // Minimum resident blocks per SM requested from the register allocator (128-thread blocks).
 #ifndef CR_TRACE_MIN_BLOCKS
-#define CR_TRACE_MIN_BLOCKS 6
+#define CR_TRACE_MIN_BLOCKS 8
 #endif
 #ifndef CR_SHADE_MIN_BLOCKS
 #define CR_SHADE_MIN_BLOCKS 4

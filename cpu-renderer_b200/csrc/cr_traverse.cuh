@@ -293,6 +293,11 @@ CR_D bool tri_reject_fast(const FastSetup& F, float4 p0, float4 p1, float4 p2) {
     return (w0 < -dw || w1 < -dw || w2 < -dw) && (w0 > dw || w1 > dw || w2 > dw);
 }
 
+// The fast traversal in the "while-while" form of Aila and Laine ("Understanding the
+// Efficiency of Ray Traversal on GPUs", HPG 2009): an inner loop walks interior nodes and
+// postpones the first leaf it reaches, continuing speculatively until every lane of the warp
+// holds a leaf; then all lanes test their leaf's triangles together. Lanes therefore run the
+// node code and the triangle code in separate loops instead of alternating per iteration.
 template <bool ANY, bool COUNT = false>
 __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore,
                                HitRec& hit, int& err, VisitCount* vc = nullptr) {
@@ -308,39 +313,22 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
     uint32_t stRef[kStackSize], stCnt[kStackSize];
     float stNear[kStackSize];
     int size = 0;
-    uint32_t ref = S.root_ref, cnt = S.root_count;
-    bool found = false, haveNode = true;
+    uint32_t ref = S.root_ref, cnt = S.root_count;   // current node (interior: cnt == 0)
+    bool haveNode = true;
+    uint32_t leafRef = 0, leafCnt = 0;               // postponed leaf
+    bool found = false;
     double bestW1 = 0, bestW2 = 0, bestDet = 1;
-    while (true) {
-        if (!haveNode) {
-            if (size == 0) break;
+    // next stack entry whose entry distance is still inside the current interval
+    auto pop = [&]() -> bool {
+        while (size > 0) {
             --size;
-            if (stNear[size] > ctmax) continue;
-            ref = stRef[size]; cnt = stCnt[size];
+            if (stNear[size] <= ctmax) { ref = stRef[size]; cnt = stCnt[size]; return true; }
         }
-        haveNode = false;
-        if (cnt) {
-            for (uint32_t i = ref; i < ref + cnt; ++i) {
-                const float4* q = S.tri_pos + 3 * static_cast<uint64_t>(i);
-                const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
-                if (COUNT) ++vc->tris;
-                const uint32_t index = __float_as_uint(q0.w);
-                if (index == ignore) continue;
-                if (tri_reject_fast(F, q0, q1, q2)) continue;
-                const double limit = smin(static_cast<double>(ctmax), closestLimit);
-                if (limit < ray.tmin) continue;
-                double t, w1, w2, det;
-                if (!tri_exact(E, v3(q0), v3(q1), v3(q2), ray.tmin, limit, t, w1, w2, det)) continue;
-                if (!accepts(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
-                if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; hit.flags = __float_as_uint(q1.w); return true; }
-                if (!found || t < hit.t || (t == hit.t && index < hit.tri)) {
-                    hit.t = t; hit.tri = index; hit.flags = __float_as_uint(q1.w); bestW1 = w1; bestW2 = w2; bestDet = det;
-                    closestLimit = t;
-                    ctmax = smin(queryLimit, next_up(static_cast<float>(t)));
-                    found = true;
-                }
-            }
-        } else {
+        return false;
+    };
+    for (;;) {
+        if (haveNode && cnt && !leafCnt) { leafRef = ref; leafCnt = cnt; haveNode = pop(); }
+        while (haveNode && cnt == 0) {
             float4 a, b, c; uint4 d;
             load_pair(S.pairs, ref, a, b, c, d);
             if (COUNT) ++vc->pairs;
@@ -353,10 +341,33 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
                 stRef[size] = firstNear ? d.z : d.x; stCnt[size] = firstNear ? d.w : d.y;
                 stNear[size] = firstNear ? n1 : n0; ++size;
                 ref = firstNear ? d.x : d.z; cnt = firstNear ? d.y : d.w;
-                haveNode = true;
-            } else if (h0) { ref = d.x; cnt = d.y; haveNode = true; }
-            else if (h1) { ref = d.z; cnt = d.w; haveNode = true; }
+            } else if (h0) { ref = d.x; cnt = d.y; }
+            else if (h1) { ref = d.z; cnt = d.w; }
+            else haveNode = pop();
+            if (haveNode && cnt && !leafCnt) { leafRef = ref; leafCnt = cnt; haveNode = pop(); }
+            if (__all_sync(__activemask(), leafCnt != 0)) break;
         }
+        for (; leafCnt; ++leafRef, --leafCnt) {
+            const float4* q = S.tri_pos + 3 * static_cast<uint64_t>(leafRef);
+            const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+            if (COUNT) ++vc->tris;
+            const uint32_t index = __float_as_uint(q0.w);
+            if (index == ignore) continue;
+            if (tri_reject_fast(F, q0, q1, q2)) continue;
+            const double limit = smin(static_cast<double>(ctmax), closestLimit);
+            if (limit < ray.tmin) continue;
+            double t, w1, w2, det;
+            if (!tri_exact(E, v3(q0), v3(q1), v3(q2), ray.tmin, limit, t, w1, w2, det)) continue;
+            if (!accepts(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
+            if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; hit.flags = __float_as_uint(q1.w); return true; }
+            if (!found || t < hit.t || (t == hit.t && index < hit.tri)) {
+                hit.t = t; hit.tri = index; hit.flags = __float_as_uint(q1.w); bestW1 = w1; bestW2 = w2; bestDet = det;
+                closestLimit = t;
+                ctmax = smin(queryLimit, next_up(static_cast<float>(t)));
+                found = true;
+            }
+        }
+        if (!haveNode) break;
     }
     if (found) { hit.u = bestW1 / bestDet; hit.v = bestW2 / bestDet; }
     return found;

@@ -165,6 +165,7 @@ def _load():
         "cr_gpu_render": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), PROGRESS_FN, P, P, C.POINTER(Stats), C.POINTER(Tuning)]),
         "cr_gpu_render_resident": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.POINTER(Stats), C.POINTER(Tuning), P]),
         "cr_gpu_film_download": (C.c_int, [P, P, C.c_uint64]),
+        "cr_gpu_render_noalloc": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), P, C.POINTER(Stats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1087,6 +1087,188 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     if (progress) progress(total, total, seconds, user);
 }
 
+// ---- allocation-free render ----------------------------------------------------------------
+// cr_gpu_render_noalloc renders through the same kernels as cr_gpu_render, but every buffer a
+// render needs beyond the scene (path pool, queues, per-sample radiance, FP64 sums, film,
+// counters) is carved out of one fixed array in device memory, so the call never allocates.
+// Every GPU that loads this library holds the array until the process exits.
+constexpr size_t kNoAllocBytes = size_t{32} << 20;          // 32 MiB per device
+constexpr uint32_t kNoAllocPool = 32768;                   // path slots
+constexpr uint64_t kNoAllocChunk = uint64_t{1} << 19;      // sample ids per chunk
+constexpr uint64_t kNoAllocMaxPixels = 512 * 512;          // largest width*height
+static __device__ __align__(256) unsigned char g_noallocScratch[kNoAllocBytes];
+
+struct NoAllocLayout {
+    PathSoA st;
+    Queues q;
+    unsigned long long* stats;
+    DevError* detail;
+    double* acc;
+    float* film;
+};
+// Lays the workspace out from `base`; returns the bytes used (the same for every call).
+size_t layoutNoAlloc(unsigned char* base, NoAllocLayout& L) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base ? base + off : nullptr;
+        off = (off + bytes + 255) / 256 * 256;
+        return static_cast<void*>(p);
+    };
+    const size_t n = kNoAllocPool;
+    PathSoA& st = L.st;
+    st.ray_o = static_cast<float4*>(take(16 * n)); st.ray_d = static_cast<float4*>(take(16 * n));
+    st.ray_lo = static_cast<float4*>(take(16 * n)); st.hit_tri = static_cast<uint32_t*>(take(4 * n));
+    st.thr = static_cast<float4*>(take(16 * n)); st.rad = static_cast<float4*>(take(16 * n));
+    st.last_pos = static_cast<float4*>(take(16 * n)); st.absorb = static_cast<float4*>(take(16 * n));
+    st.flags = static_cast<uint32_t*>(take(4 * n)); st.rng = static_cast<uint64_t*>(take(8 * n));
+    st.prev_tri = static_cast<uint32_t*>(take(4 * n)); st.pixel = static_cast<uint32_t*>(take(4 * n));
+    st.sample = static_cast<uint32_t*>(take(4 * n)); st.depth = static_cast<uint32_t*>(take(4 * n));
+    st.sh_o = static_cast<float4*>(take(16 * n)); st.sh_d = static_cast<float4*>(take(16 * n));
+    st.sh_lo = static_cast<float4*>(take(16 * n)); st.sh_c = static_cast<float4*>(take(16 * n));
+    st.out = static_cast<float4*>(take(16 * kNoAllocChunk));
+    for (int k = 0; k < 2; ++k) {
+        L.q.extend[k] = static_cast<uint32_t*>(take(4 * n));
+        L.q.shadow[k] = static_cast<uint32_t*>(take(4 * n));
+        L.q.free[k] = static_cast<uint32_t*>(take(4 * n));
+    }
+    for (int c = 0; c < kShadeClasses; ++c) L.q.shade[c] = static_cast<uint32_t*>(take(4 * n));
+    L.q.counts = static_cast<uint32_t*>(take(4 * kCountWords));
+    L.stats = static_cast<unsigned long long*>(take(8 * kStatWords));
+    L.detail = static_cast<DevError*>(take(sizeof(DevError)));
+    L.acc = static_cast<double*>(take(24 * kNoAllocMaxPixels));
+    L.film = static_cast<float*>(take(12 * kNoAllocMaxPixels));
+    return off;
+}
+
+// Device address of the workspace, looked up once per device (cudaGetSymbolAddress) with that
+// device current; the host-side name of the array is not a device address.
+unsigned char* noallocBase(int device) {
+    static std::mutex m;
+    static unsigned char* addr[64] = {};
+    if (device < 0 || device >= 64) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "device index out of range");
+    std::lock_guard<std::mutex> lock(m);
+    if (!addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+        if (e != cudaSuccess) throw CudaError(e, "cudaGetSymbolAddress(g_noallocScratch)");
+        addr[device] = static_cast<unsigned char*>(p);
+    }
+    return addr[device];
+}
+
+void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, float* filmHost,
+                   cr_render_stats* stats) {
+    const auto start = std::chrono::steady_clock::now();
+    crh::validate_options(o);
+    const uint64_t pixels = static_cast<uint64_t>(o.width) * o.height;
+    if (pixels > kNoAllocMaxPixels)
+        throw crh::Error(CR_ERR_INVALID_ARGUMENT, "cr_gpu_render_noalloc: width*height " + std::to_string(pixels) +
+                                                      " exceeds its fixed workspace limit of 262144 pixels (512x512)");
+    const uint64_t total = pixels * static_cast<uint64_t>(o.samples);
+    const cr_gpu_tuning tuning{};
+    RenderParams P;
+    try {
+        P = makeParams(g, camera, o, tuning);
+    } catch (const crh::Error& e) {
+        throw crh::Error(CR_ERR_RENDER, std::string("Pixel (0,0), sample 0: ") + e.what());
+    }
+    CR_CUDA(cudaSetDevice(g.device));
+    NoAllocLayout L;
+    if (layoutNoAlloc(nullptr, L) > kNoAllocBytes) throw crh::Error(CR_ERR_LOGIC, "no-alloc workspace layout exceeds its array");
+    layoutNoAlloc(noallocBase(g.device), L);
+    cudaStream_t s = g.stream;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
+    const int gridTrace = occupancyGrid(reinterpret_cast<const void*>(k_trace<false>), 128, g.device);
+    const int gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
+    const int gridLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
+    const int gridMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
+    const int gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen), 128, g.device);
+    const int gridSmall = sms * 8;
+    // The workspace keeps the previous call's contents: clear what must start at zero.
+    CR_CUDA(cudaMemsetAsync(L.acc, 0, 3 * pixels * sizeof(double), s));
+    CR_CUDA(cudaMemsetAsync(L.stats, 0, kStatWords * sizeof(unsigned long long), s));
+    const unsigned long long noError = ~0ull;
+    CR_CUDA(cudaMemcpyAsync(L.stats + kStatErrorKey, &noError, sizeof(noError), cudaMemcpyHostToDevice, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    const ErrSink E{L.stats + kStatErrorKey, nullptr};
+    uint32_t hostCounts[kCountWords];
+    unsigned long long hostStats[kStatWords];
+    const uint64_t pool = std::min<uint64_t>(kNoAllocPool, total);
+    const uint64_t chunk = std::min<uint64_t>(total, kNoAllocChunk);
+    uint64_t iterations = 0, launches = 0;
+    bool errored = false;
+    for (uint64_t c0 = 0; c0 < total && !errored; c0 += chunk) {
+        const Chunk C{c0, std::min<uint64_t>(total, c0 + chunk), pixels};
+        CR_CUDA(cudaMemsetAsync(L.q.counts, 0, kCountWords * sizeof(uint32_t), s));
+        const unsigned long long issuedStart = c0;
+        CR_CUDA(cudaMemcpyAsync(L.stats + kStatIssued, &issuedStart, sizeof(issuedStart), cudaMemcpyHostToDevice, s));
+        k_pool_init<<<gridSmall, 128, 0, s>>>(L.q, static_cast<uint32_t>(pool));
+        ++launches;
+        const uint64_t maxIterations = ((C.c1 - C.c0) / pool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
+        uint64_t iter = 0;
+        int cur = 0;
+        for (;;) {
+            for (int b = 0; b < 8; ++b) {
+                k_regen<<<gridRegen, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
+                k_trace<false><<<gridTrace, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
+                k_shade<kShadeMiss><<<gridMiss, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
+                k_shade<kShadeNeeNull><<<gridLight, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
+                k_shade<kShadeGeneric><<<gridShade, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
+                launches += 5;
+                cur ^= 1;
+                ++iter;
+                ++iterations;
+            }
+            CR_CUDA(cudaMemcpyAsync(hostCounts, L.q.counts, sizeof(hostCounts), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaMemcpyAsync(hostStats, L.stats, sizeof(hostStats), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaStreamSynchronize(s));
+            CR_CUDA(cudaGetLastError());
+            const uint64_t live = hostCounts[kCountExtend0 + cur] + hostCounts[kCountShadow0 + (cur ^ 1)];
+            if (hostStats[kStatErrorKey] != ~0ull) { errored = true; break; }
+            if (hostStats[kStatIssued] >= C.c1 && live == 0) break;
+            if (iter > maxIterations) throw crh::Error(CR_ERR_DEVICE_TIMEOUT, "paths still live after the iteration bound");
+        }
+        if (errored) break;
+        k_accumulate<<<gridSmall, 128, 0, s>>>(L.st.out, C, L.acc);
+        ++launches;
+    }
+    if (errored) {
+        const unsigned long long key = hostStats[kStatErrorKey];
+        const uint32_t sample = static_cast<uint32_t>(key & ((1ull << 21) - 1));
+        const uint64_t rank = key >> 21, tilesX = (static_cast<uint64_t>(o.width) + 15) / 16;
+        const uint64_t tile = rank / 256, within = rank % 256;
+        const uint32_t x = static_cast<uint32_t>((tile % tilesX) * 16 + within % 16);
+        const uint32_t y = static_cast<uint32_t>((tile / tilesX) * 16 + within / 16);
+        DevError host{};
+        CR_CUDA(cudaMemsetAsync(L.detail, 0, sizeof(DevError), s));
+        CR_CUDA(cudaMemsetAsync(L.stats, 0, 2 * sizeof(unsigned long long), s));
+        k_trace_one<<<1, 32, 0, s>>>(g.dev, P, L.st, y * static_cast<uint32_t>(o.width) + x, sample, L.detail, L.stats, L.stats + 1);
+        CR_CUDA(cudaMemcpyAsync(&host, L.detail, sizeof(DevError), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        if (!host.code) { host.code = -1; host.x = static_cast<int32_t>(x); host.y = static_cast<int32_t>(y); host.sample = static_cast<int32_t>(sample); }
+        throw crh::Error(CR_ERR_RENDER, crh::sample_error_message(host));
+    }
+    k_film<<<gridSmall, 128, 0, s>>>(L.acc, L.film, pixels, o.samples);
+    ++launches;
+    if (filmHost) CR_CUDA(cudaMemcpyAsync(filmHost, L.film, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaMemcpyAsync(hostStats, L.stats, sizeof(hostStats), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    CR_CUDA(cudaGetLastError());
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+        stats->workers = referenceWorkers(o);
+        stats->chunks = static_cast<int32_t>((total + chunk - 1) / chunk);
+        stats->camera_samples = total;
+        stats->boundary_retries = hostStats[kStatRetries];
+        stats->extend_rays = hostStats[kStatExtendRays];
+        stats->shadow_rays = hostStats[kStatShadowRays];
+        stats->kernel_launches = launches;
+        stats->iterations = iterations;
+    }
+}
+
 cr_gpu_tuning defaults(const cr_gpu_tuning* t) {
     cr_gpu_tuning d{};
     if (t) d = *t;
@@ -1209,6 +1391,16 @@ cr_status cr_gpu_render_resident(cr_gpu_scene* g, const cr_camera* camera, const
         if (!g || !camera || !options) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
         std::lock_guard<std::mutex> lock(g->mutex);
         renderImpl(*g, *camera, *options, nullptr, nullptr, nullptr, stats, defaults(tuning), per_sample_rgb);
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_render_noalloc(cr_gpu_scene* g, const cr_camera* camera, const cr_render_options* options,
+                                float* film_rgb, cr_render_stats* stats) {
+    try {
+        if (!g || !camera || !options) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        renderNoAlloc(*g, *camera, *options, film_rgb, stats);
         return CR_OK;
     } catch (const std::exception& e) { return fail(e); }
 }

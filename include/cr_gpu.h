@@ -296,6 +296,29 @@ cr_status cr_gpu_render_resident(cr_gpu_scene* scene, const cr_camera* camera,
                                  const cr_gpu_tuning* tuning, float* per_sample_rgb);
 cr_status cr_gpu_film_download(cr_gpu_scene* scene, float* film_rgb, uint64_t floats);
 
+/* cr_gpu_render without any allocation (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory while rendering: hosts that hand out GPU
+ * memory only at start-up (fixed budgets or their own pools), request paths that must not
+ * block on cudaMalloc/cudaFree (both may synchronise the device and can fail under memory
+ * pressure mid-request), and code that must not fragment a shared device. Everything the
+ * render needs besides the scene (created earlier with cr_gpu_scene_create) comes from one
+ * fixed 32 MiB array in device memory that every GPU loading this library holds until the
+ * process exits; film_rgb (host memory, width*height*3 floats) receives the same film
+ * cr_gpu_render produces.
+ *
+ * Limits: width*height <= 262144 (512x512); any sample and bounce counts cr::RenderOptions
+ * accepts. Larger images fail with CR_ERR_INVALID_ARGUMENT before any work.
+ *
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture. All calls on a device share the array and
+ * it keeps the last call's contents (each call clears what must start at zero); calls that
+ * overlap on the GPU — from different threads or scenes on one device — race on it and must
+ * be serialised by the caller. */
+cr_status cr_gpu_render_noalloc(cr_gpu_scene* scene, const cr_camera* camera,
+                                const cr_render_options* options, float* film_rgb,
+                                cr_render_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,12 +10,14 @@
 #include "cr_host.h"
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cmath>
 #include <cstring>
 #include <limits>
 #include <numeric>
 #include <sstream>
+#include <thread>
 
 namespace crh {
 namespace {
@@ -373,7 +375,20 @@ void build_bvh(const cr_triangle* triangles, uint64_t count, std::vector<cr_bvh_
     b.subdivide(0, 0, static_cast<uint32_t>(count), 0);
 }
 
-void build_environment(const cr_environment_desc& e, EnvTables& out) {
+void parallel_for(uint64_t n, const std::function<void(uint64_t, uint64_t)>& fn, uint64_t grain) {
+    const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t parts = std::min<uint64_t>(hw, (n + grain - 1) / std::max<uint64_t>(1, grain));
+    if (parts <= 1) { if (n) fn(0, n); return; }
+    std::vector<std::thread> pool;
+    pool.reserve(parts);
+    for (uint64_t k = 0; k < parts; ++k) {
+        const uint64_t b = n * k / parts, e = n * (k + 1) / parts;
+        pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    for (auto& t : pool) t.join();
+}
+
+void build_environment(const cr_environment_desc& e, EnvTables& out, bool alias) {
     out = EnvTables{};
     if (!e.pixels) {  // Environment(Vec3) (render.cpp:12-14)
         const Vec3 c = v3(e.constant);
@@ -394,20 +409,30 @@ void build_environment(const cr_environment_desc& e, EnvTables& out) {
         const double a = static_cast<double>(pi) * row / H, b = static_cast<double>(pi) * (row + 1) / H;
         return (2 * static_cast<double>(pi) / W) * (std::cos(a) - std::cos(b));
     };
-    out.cdf.reserve(n);
     std::vector<double> omegas(H);
-    for (int y = 0; y < H; ++y) {
-        const double omega = solidAngle(y);
-        omegas[y] = omega;
-        for (int x = 0; x < W; ++x) {
-            const float* p = e.pixels + 4 * (static_cast<size_t>(y) * W + x);
+    for (int y = 0; y < H; ++y) omegas[y] = solidAngle(y);
+    // Texel weights in parallel; the running sums below stay sequential, in the reference's
+    // order, so the CDF is bit-identical (render.cpp:29-41).
+    std::vector<double> light(n);
+    std::atomic<bool> bad{false};
+    parallel_for(n, [&](uint64_t b, uint64_t en) {
+        for (uint64_t i = b; i < en; ++i) {
+            const float* p = e.pixels + 4 * i;
             const Vec3 color{p[0], p[1], p[2]};
-            if (!finite(color) || std::min({p[0], p[1], p[2]}) < 0)
-                throw Error(CR_ERR_INVALID_ARGUMENT, "Non-finite or negative HDR environment pixel");
-            const double light = luminance(color) * out.intensity;
-            out.integral += light * omega;
-            out.weightSum += (light + 1e-9) * omega;
-            out.cdf.push_back(out.weightSum);
+            if (!finite(color) || std::min({p[0], p[1], p[2]}) < 0) bad = true;
+            light[i] = luminance(color) * out.intensity;
+        }
+    });
+    if (bad) throw Error(CR_ERR_INVALID_ARGUMENT, "Non-finite or negative HDR environment pixel");
+    out.cdf.resize(n);
+    for (int y = 0; y < H; ++y) {
+        const double omega = omegas[y];
+        const size_t row = static_cast<size_t>(y) * W;
+        for (int x = 0; x < W; ++x) {
+            const double l = light[row + x];
+            out.integral += l * omega;
+            out.weightSum += (l + 1e-9) * omega;
+            out.cdf[row + x] = out.weightSum;
         }
     }
     if (e.cdf) {  // the caller's own copy of the same table
@@ -416,21 +441,30 @@ void build_environment(const cr_environment_desc& e, EnvTables& out) {
     }
     // Per-texel density as Environment::pdf/sample evaluate it (render.cpp:82, 93).
     out.pdf.resize(n);
-    for (size_t i = 0; i < n; ++i) {
-        const int y = static_cast<int>(i / W);
-        out.pdf[i] = static_cast<float>((out.cdf[i] - (i ? out.cdf[i - 1] : 0)) / (out.weightSum * omegas[y]));
-    }
+    parallel_for(n, [&](uint64_t b, uint64_t en) {
+        for (uint64_t i = b; i < en; ++i) {
+            const int y = static_cast<int>(i / W);
+            out.pdf[i] = static_cast<float>((out.cdf[i] - (i ? out.cdf[i - 1] : 0)) / (out.weightSum * omegas[y]));
+        }
+    });
     out.rowCos.resize(H + 1);
     for (int y = 0; y <= H; ++y) out.rowCos[y] = std::cos(pi * static_cast<float>(y) / static_cast<float>(H));
     // Bracket table: upper_bound of j*weightSum/K.
     uint32_t K = 1;
     while (K < n / 32 && K < (1u << 16)) K <<= 1;
     out.coarse.resize(K);
-    for (uint32_t j = 0; j < K; ++j) {
-        const double pick = out.weightSum * (static_cast<double>(j) / K);
-        out.coarse[j] = static_cast<uint32_t>(std::upper_bound(out.cdf.begin(), out.cdf.end(), pick) - out.cdf.begin());
-    }
-    // Alias table (Vose's method) over the same texel probabilities.
+    parallel_for(K, [&](uint64_t b, uint64_t en) {
+        for (uint64_t j = b; j < en; ++j) {
+            const double pick = out.weightSum * (static_cast<double>(j) / K);
+            out.coarse[j] = static_cast<uint32_t>(std::upper_bound(out.cdf.begin(), out.cdf.end(), pick) - out.cdf.begin());
+        }
+    }, 4096);
+    if (alias) build_alias(out);
+}
+
+void build_alias(EnvTables& out) {
+    if (!out.hasImage || !out.aliasProb.empty()) return;
+    const size_t n = out.cdf.size();
     out.aliasProb.assign(n, 1.0f);
     out.aliasIndex.resize(n);
     std::vector<double> scaled(n);
@@ -441,11 +475,11 @@ void build_environment(const cr_environment_desc& e, EnvTables& out) {
         (scaled[i] < 1.0 ? small : large).push_back(static_cast<uint32_t>(i));
     }
     while (!small.empty() && !large.empty()) {
-        const uint32_t s = small.back(); small.pop_back();
+        const uint32_t sm = small.back(); small.pop_back();
         const uint32_t l = large.back();
-        out.aliasProb[s] = static_cast<float>(scaled[s]);
-        out.aliasIndex[s] = l;
-        scaled[l] = (scaled[l] + scaled[s]) - 1.0;
+        out.aliasProb[sm] = static_cast<float>(scaled[sm]);
+        out.aliasIndex[sm] = l;
+        scaled[l] = (scaled[l] + scaled[sm]) - 1.0;
         if (scaled[l] < 1.0) { large.pop_back(); small.push_back(l); }
     }
 }

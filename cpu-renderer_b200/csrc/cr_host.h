@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <functional>
 #include <vector>
 #include "cr_gpu.h"
 #include "cr_internal.h"
@@ -43,7 +44,12 @@ struct EnvTables {
     std::vector<float> aliasProb;
     std::vector<uint32_t> aliasIndex;
 };
-void build_environment(const cr_environment_desc& e, EnvTables& out);
+void build_environment(const cr_environment_desc& e, EnvTables& out, bool alias = false);
+// Walker/Vose alias table over the same texel probabilities (built on demand).
+void build_alias(EnvTables& t);
+
+// Runs fn(begin, end) over [0, n) split across the host's hardware threads.
+void parallel_for(uint64_t n, const std::function<void(uint64_t, uint64_t)>& fn, uint64_t grain = 65536);
 
 // Lights (render.cpp:131-160).
 struct LightTables {

@@ -20,6 +20,7 @@
 #include "cr_shade.cuh"
 #include "cr_host.h"
 
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <memory>
@@ -595,46 +596,25 @@ int occupancyGrid(const void* kernel, int block, int device) {
 
 }  // namespace
 
-struct cr_gpu_scene {
+// Render work buffers of one device: the path pool, its queues, the chunk's per-sample
+// radiance and the host staging words. Kept for the life of the process and shared by every
+// scene on the device (a render holds the mutex), so a new scene does not pay for fresh
+// multi-gigabyte allocations.
+struct Workspace {
     int device = 0;
-    cudaStream_t stream = nullptr;
-    DevAlloc geometry;  // scene data
-    DevAlloc work;      // path buffers
-    DevScene dev{};
-    uint64_t triangleCount = 0;
-    // work buffers: the path pool, its queues, and the chunk's per-sample output
-    size_t capacity = 0;        // pool slots
-    size_t outCapacity = 0;     // samples per chunk
+    std::mutex mutex;
+    DevAlloc work, outAlloc, packedAlloc;
+    size_t capacity = 0, outCapacity = 0, packedCapacity = 0;
     PathSoA st{};
     Queues q{};
     uint32_t* counts = nullptr;
     unsigned long long* stats = nullptr;
     DevError* detail = nullptr;
-    double* acc = nullptr;
-    float* film = nullptr;
-    float* packed = nullptr;    // per-sample RGB staging for stream dumps
-    size_t packedCapacity = 0;
-    size_t filmPixels = 0;
-    DevAlloc filmAlloc, outAlloc, packedAlloc;
+    float* packed = nullptr;
     uint32_t* hostCounts = nullptr;           // pinned
     unsigned long long* hostStats = nullptr;  // pinned
     int gridTrace = 0, gridShade = 0, gridShadeLight = 0, gridShadeMiss = 0, gridRegen = 0, gridSmall = 0;
     std::vector<cudaEvent_t> events;
-    std::mutex mutex;
-
-    ~cr_gpu_scene() {
-        if (device >= 0) cudaSetDevice(device);
-        for (cudaEvent_t e : events) cudaEventDestroy(e);
-        if (stream) cudaStreamSynchronize(stream);
-        geometry.release();
-        work.release();
-        filmAlloc.release();
-        outAlloc.release();
-        packedAlloc.release();
-        if (hostCounts) cudaFreeHost(hostCounts);
-        if (hostStats) cudaFreeHost(hostStats);
-        if (stream) cudaStreamDestroy(stream);
-    }
 
     cudaEvent_t event(size_t i) {
         while (events.size() <= i) {
@@ -644,11 +624,10 @@ struct cr_gpu_scene {
         }
         return events[i];
     }
-
     void ensureWork(size_t paths) {
         if (paths <= capacity) return;
-        CR_CUDA(cudaStreamSynchronize(stream));
         work.release();
+        capacity = 0;
         const size_t n = paths;
         st.ray_o = work.alloc<float4>(n); st.ray_d = work.alloc<float4>(n); st.ray_lo = work.alloc<float4>(n);
         st.hit_tri = work.alloc<uint32_t>(n);
@@ -670,27 +649,63 @@ struct cr_gpu_scene {
         detail = work.alloc<DevError>(1);
         capacity = n;
     }
-
     void ensureOut(size_t samples) {
         if (samples <= outCapacity) return;
-        CR_CUDA(cudaStreamSynchronize(stream));
         outAlloc.release();
+        outCapacity = 0;
         st.out = outAlloc.alloc<float4>(samples);
         outCapacity = samples;
     }
-
     void ensurePacked(size_t samples) {
         if (samples <= packedCapacity) return;
-        CR_CUDA(cudaStreamSynchronize(stream));
         packedAlloc.release();
+        packedCapacity = 0;
         packed = packedAlloc.alloc<float>(3 * samples);
         packedCapacity = samples;
+    }
+    uint64_t bytes() const { return work.bytes + outAlloc.bytes + packedAlloc.bytes; }
+};
+
+// One workspace per device, created on first use and intentionally never destroyed (process
+// exit reclaims device memory; destroying after the CUDA runtime has shut down would fail).
+Workspace& workspaceFor(int device) {
+    static std::mutex m;
+    static Workspace* ws[64] = {};
+    if (device < 0 || device >= 64) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "device index out of range");
+    std::lock_guard<std::mutex> lock(m);
+    if (!ws[device]) { ws[device] = new Workspace; ws[device]->device = device; }
+    return *ws[device];
+}
+
+struct cr_gpu_scene {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevAlloc geometry;  // scene data
+    DevScene dev{};
+    uint64_t triangleCount = 0;
+    crh::EnvTables env;  // host copy, for the alias table built on demand
+    DevAlloc aliasAlloc;
+    // film of the last render: FP64 sums and the float film
+    double* acc = nullptr;
+    float* film = nullptr;
+    size_t filmPixels = 0;
+    DevAlloc filmAlloc;
+    std::mutex mutex;
+
+    ~cr_gpu_scene() {
+        if (device >= 0) cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        geometry.release();
+        aliasAlloc.release();
+        filmAlloc.release();
+        if (stream) cudaStreamDestroy(stream);
     }
 
     void ensureFilm(size_t pixels) {
         if (pixels <= filmPixels) return;
         CR_CUDA(cudaStreamSynchronize(stream));
         filmAlloc.release();
+        filmPixels = 0;
         acc = filmAlloc.alloc<double>(3 * pixels);
         film = filmAlloc.alloc<float>(3 * pixels);
         filmPixels = pixels;
@@ -710,8 +725,14 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     const uint64_t n = d.triangle_count;
     if (n && !d.triangles) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "triangles is NULL");
     if (d.material_count && !d.materials) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "materials is NULL");
-    for (uint64_t i = 0; i < n; ++i)
-        if (d.triangles[i].material >= d.material_count) throw crh::Error(CR_ERR_OUT_OF_RANGE, "Triangle material index out of range");
+    {
+        std::atomic<bool> bad{false};
+        crh::parallel_for(n, [&](uint64_t b, uint64_t e) {
+            for (uint64_t i = b; i < e; ++i)
+                if (d.triangles[i].material >= d.material_count) bad = true;
+        });
+        if (bad) throw crh::Error(CR_ERR_OUT_OF_RANGE, "Triangle material index out of range");
+    }
     for (uint32_t m = 0; m < d.material_count; ++m) {
         const cr_material& mat = d.materials[m];
         const cr_texture_slot* s[5] = {&mat.base_color_texture, &mat.metallic_roughness_texture, &mat.normal_texture,
@@ -737,15 +758,25 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
         crh::build_bvh(d.triangles, n, nodes, indices);
     }
     // Structure checks: adjacent children at odd indices, leaf ranges inside indices.
-    for (size_t i = 0; i < nodes.size(); ++i) {
-        const cr_bvh_node& nd = nodes[i];
-        if (nd.count) {
-            if (static_cast<uint64_t>(nd.first) + nd.count > indices.size()) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH leaf range outside its index array");
-        } else if ((nd.first & 1u) == 0 || static_cast<uint64_t>(nd.first) + 1 >= nodes.size() || nd.first <= i) {
-            throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH interior node does not reference an adjacent child pair");
-        }
+    {
+        std::atomic<int> bad{0};
+        crh::parallel_for(nodes.size(), [&](uint64_t b, uint64_t e) {
+            for (uint64_t i = b; i < e; ++i) {
+                const cr_bvh_node& nd = nodes[i];
+                if (nd.count) {
+                    if (static_cast<uint64_t>(nd.first) + nd.count > indices.size()) bad = 1;
+                } else if ((nd.first & 1u) == 0 || static_cast<uint64_t>(nd.first) + 1 >= nodes.size() || nd.first <= i) {
+                    bad = 2;
+                }
+            }
+        });
+        if (bad == 1) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH leaf range outside its index array");
+        if (bad == 2) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH interior node does not reference an adjacent child pair");
+        crh::parallel_for(indices.size(), [&](uint64_t b, uint64_t e) {
+            for (uint64_t i = b; i < e; ++i) if (indices[i] >= n) bad = 3;
+        });
+        if (bad == 3) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH index outside the triangle array");
     }
-    for (uint32_t idx : indices) if (idx >= n) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH index outside the triangle array");
 
     cudaStream_t s = g.stream;
     DevScene& S = g.dev;
@@ -755,69 +786,80 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     // per-triangle flags and geometric normals (Scene::accepts, geometry.cpp:282-290)
     std::vector<float4> ng(n ? n : 1);
     std::vector<uint32_t> flags(n ? n : 1, 0);
-    uint32_t anyMask = 0;
-    bool texturedEmitter = false;
-    for (uint64_t i = 0; i < n; ++i) {
-        const cr_triangle& t = d.triangles[i];
-        const cr_material& m = d.materials[t.material];
-        uint32_t f = 0;
-        if (!m.double_sided && m.transmission <= 0) f |= kTriCull;
-        if (m.alpha_mode == CR_ALPHA_MASK) { f |= kTriAlphaMask; anyMask = 1; }
-        // bsdf.cpp:171-179: smooth, and the diffuse weight (1-metallic)(1-transmission) is zero
-        if (m.roughness <= 0.001f && m.metallic_roughness_texture.texture < 0 &&
-            (m.metallic == 1.0f || (m.transmission == 1.0f && m.transmission_texture.texture < 0)))
-            f |= kTriNeeNull;
-        const bool textured = m.base_color_texture.texture >= 0 || m.metallic_roughness_texture.texture >= 0 ||
-                              m.normal_texture.texture >= 0 || m.emissive_texture.texture >= 0 ||
-                              m.transmission_texture.texture >= 0;
-        if (textured && (m.emission[0] > 0 || m.emission[1] > 0 || m.emission[2] > 0)) texturedEmitter = true;
-        flags[i] = f;
-        float gx = t.geometric_normal[0], gy = t.geometric_normal[1], gz = t.geometric_normal[2];
-        if (gx == 0 && gy == 0 && gz == 0) {  // geometry.cpp:284
-            const double ax = static_cast<double>(t.v[1].position[0]) - t.v[0].position[0];
-            const double ay = static_cast<double>(t.v[1].position[1]) - t.v[0].position[1];
-            const double az = static_cast<double>(t.v[1].position[2]) - t.v[0].position[2];
-            const double bx = static_cast<double>(t.v[2].position[0]) - t.v[0].position[0];
-            const double by = static_cast<double>(t.v[2].position[1]) - t.v[0].position[1];
-            const double bz = static_cast<double>(t.v[2].position[2]) - t.v[0].position[2];
-            const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
-            const double sq = cx * cx + cy * cy + cz * cz;
-            if (sq > 0 && std::isfinite(sq)) {
-                const double inv = 1 / std::sqrt(sq);
-                gx = static_cast<float>(cx * inv); gy = static_cast<float>(cy * inv); gz = static_cast<float>(cz * inv);
+    std::atomic<uint32_t> anyMaskA{0};
+    std::atomic<bool> texturedEmitterA{false};
+    crh::parallel_for(n, [&](uint64_t b, uint64_t e) {
+        uint32_t localMask = 0;
+        bool localEmitter = false;
+        for (uint64_t i = b; i < e; ++i) {
+            const cr_triangle& t = d.triangles[i];
+            const cr_material& m = d.materials[t.material];
+            uint32_t f = 0;
+            if (!m.double_sided && m.transmission <= 0) f |= kTriCull;
+            if (m.alpha_mode == CR_ALPHA_MASK) { f |= kTriAlphaMask; localMask = 1; }
+            // bsdf.cpp:171-179: smooth, and the diffuse weight (1-metallic)(1-transmission) is zero
+            if (m.roughness <= 0.001f && m.metallic_roughness_texture.texture < 0 &&
+                (m.metallic == 1.0f || (m.transmission == 1.0f && m.transmission_texture.texture < 0)))
+                f |= kTriNeeNull;
+            const bool textured = m.base_color_texture.texture >= 0 || m.metallic_roughness_texture.texture >= 0 ||
+                                  m.normal_texture.texture >= 0 || m.emissive_texture.texture >= 0 ||
+                                  m.transmission_texture.texture >= 0;
+            if (textured && (m.emission[0] > 0 || m.emission[1] > 0 || m.emission[2] > 0)) localEmitter = true;
+            flags[i] = f;
+            float gx = t.geometric_normal[0], gy = t.geometric_normal[1], gz = t.geometric_normal[2];
+            if (gx == 0 && gy == 0 && gz == 0) {  // geometry.cpp:284
+                const double ax = static_cast<double>(t.v[1].position[0]) - t.v[0].position[0];
+                const double ay = static_cast<double>(t.v[1].position[1]) - t.v[0].position[1];
+                const double az = static_cast<double>(t.v[1].position[2]) - t.v[0].position[2];
+                const double bx = static_cast<double>(t.v[2].position[0]) - t.v[0].position[0];
+                const double by = static_cast<double>(t.v[2].position[1]) - t.v[0].position[1];
+                const double bz = static_cast<double>(t.v[2].position[2]) - t.v[0].position[2];
+                const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+                const double sq = cx * cx + cy * cy + cz * cz;
+                if (sq > 0 && std::isfinite(sq)) {
+                    const double inv = 1 / std::sqrt(sq);
+                    gx = static_cast<float>(cx * inv); gy = static_cast<float>(cy * inv); gz = static_cast<float>(cz * inv);
+                }
             }
+            float fw;
+            std::memcpy(&fw, &f, 4);
+            ng[i] = make_float4(gx, gy, gz, fw);
         }
-        uint32_t fb = f;
-        float fw;
-        std::memcpy(&fw, &fb, 4);
-        ng[i] = make_float4(gx, gy, gz, fw);
-    }
+        if (localMask) anyMaskA = 1;
+        if (localEmitter) texturedEmitterA = true;
+    });
+    const uint32_t anyMask = anyMaskA;
+    const bool texturedEmitter = texturedEmitterA;
     std::vector<float4> pos(3 * (indices.empty() ? 1 : indices.size()));
-    for (size_t slot = 0; slot < indices.size(); ++slot) {
-        const uint32_t idx = indices[slot];
-        const cr_triangle& t = d.triangles[idx];
-        float w0, w1;
-        std::memcpy(&w0, &idx, 4);
-        std::memcpy(&w1, &flags[idx], 4);
-        pos[3 * slot] = make_float4(t.v[0].position[0], t.v[0].position[1], t.v[0].position[2], w0);
-        pos[3 * slot + 1] = make_float4(t.v[1].position[0], t.v[1].position[1], t.v[1].position[2], w1);
-        pos[3 * slot + 2] = make_float4(t.v[2].position[0], t.v[2].position[1], t.v[2].position[2], 0.0f);
-    }
+    crh::parallel_for(indices.size(), [&](uint64_t b, uint64_t e) {
+        for (uint64_t slot = b; slot < e; ++slot) {
+            const uint32_t idx = indices[slot];
+            const cr_triangle& t = d.triangles[idx];
+            float w0, w1;
+            std::memcpy(&w0, &idx, 4);
+            std::memcpy(&w1, &flags[idx], 4);
+            pos[3 * slot] = make_float4(t.v[0].position[0], t.v[0].position[1], t.v[0].position[2], w0);
+            pos[3 * slot + 1] = make_float4(t.v[1].position[0], t.v[1].position[1], t.v[1].position[2], w1);
+            pos[3 * slot + 2] = make_float4(t.v[2].position[0], t.v[2].position[1], t.v[2].position[2], 0.0f);
+        }
+    });
     const size_t pairCount = nodes.size() > 1 ? (nodes.size() - 1) / 2 : 0;
     std::vector<NodePair> pairs(pairCount ? pairCount : 1);
     auto childRef = [&](const cr_bvh_node& c, uint32_t& ref, uint32_t& cnt) {
         if (c.count) { ref = c.first; cnt = c.count; } else { ref = (c.first - 1) / 2; cnt = 0; }
     };
-    for (size_t p = 0; p < pairCount; ++p) {
-        const cr_bvh_node& c0 = nodes[2 * p + 1];
-        const cr_bvh_node& c1 = nodes[2 * p + 2];
-        NodePair& np = pairs[p];
-        np.a = make_float4(c0.lo[0], c0.lo[1], c0.lo[2], c0.hi[0]);
-        np.b = make_float4(c0.hi[1], c0.hi[2], c1.lo[0], c1.lo[1]);
-        np.c = make_float4(c1.lo[2], c1.hi[0], c1.hi[1], c1.hi[2]);
-        childRef(c0, np.d.x, np.d.y);
-        childRef(c1, np.d.z, np.d.w);
-    }
+    crh::parallel_for(pairCount, [&](uint64_t b, uint64_t e) {
+        for (uint64_t p = b; p < e; ++p) {
+            const cr_bvh_node& c0 = nodes[2 * p + 1];
+            const cr_bvh_node& c1 = nodes[2 * p + 2];
+            NodePair& np = pairs[p];
+            np.a = make_float4(c0.lo[0], c0.lo[1], c0.lo[2], c0.hi[0]);
+            np.b = make_float4(c0.hi[1], c0.hi[2], c1.lo[0], c1.lo[1]);
+            np.c = make_float4(c1.lo[2], c1.hi[0], c1.hi[1], c1.hi[2]);
+            childRef(c0, np.d.x, np.d.y);
+            childRef(c1, np.d.z, np.d.w);
+        }
+    });
     if (!nodes.empty()) {
         S.has_root = 1;
         for (int k = 0; k < 3; ++k) { S.root_lo[k] = nodes[0].lo[k]; S.root_hi[k] = nodes[0].hi[k]; }
@@ -855,7 +897,7 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     S.textures = g.geometry.upload(d.textures, d.texture_count, s);
     S.texture_count = d.texture_count;
     // environment
-    crh::EnvTables E;
+    crh::EnvTables& E = g.env;
     crh::build_environment(env, E);
     S.env_has_image = E.hasImage;
     for (int k = 0; k < 3; ++k) S.env_constant[k] = E.constant[k];
@@ -868,8 +910,8 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
         S.env_row_cos = g.geometry.upload(E.rowCos.data(), E.rowCos.size(), s);
         S.env_coarse = g.geometry.upload(E.coarse.data(), E.coarse.size(), s);
         S.env_coarse_count = static_cast<uint32_t>(E.coarse.size());
-        S.alias_prob = g.geometry.upload(E.aliasProb.data(), E.aliasProb.size(), s);
-        S.alias_index = g.geometry.upload(E.aliasIndex.data(), E.aliasIndex.size(), s);
+        S.alias_prob = nullptr;  // built on the first render that asks for alias sampling
+        S.alias_index = nullptr;
     }
     S.env_weight_sum = E.weightSum;
     S.env_rotation = E.rotation;
@@ -934,34 +976,41 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     pool = (pool + 127) / 128 * 128;
     const uint64_t chunkBudget = uint64_t{1} << 28;  // 268 M samples = 4 GiB of float4 radiance
     const uint64_t chunk = std::min<uint64_t>(total, std::max<uint64_t>(pool, chunkBudget));
-    g.ensureWork(static_cast<size_t>(pool));
-    g.ensureOut(static_cast<size_t>(chunk));
+    Workspace& W = workspaceFor(g.device);
+    std::lock_guard<std::mutex> wsLock(W.mutex);
+    W.ensureWork(static_cast<size_t>(pool));
+    W.ensureOut(static_cast<size_t>(chunk));
     g.ensureFilm(pixels);
-    if (perSample) g.ensurePacked(static_cast<size_t>(chunk));
-    if (!g.hostCounts) CR_CUDA(cudaMallocHost(&g.hostCounts, kCountWords * sizeof(uint32_t)));
-    if (!g.hostStats) CR_CUDA(cudaMallocHost(&g.hostStats, kStatWords * sizeof(unsigned long long)));
+    if (perSample) W.ensurePacked(static_cast<size_t>(chunk));
+    if (!W.hostCounts) CR_CUDA(cudaMallocHost(&W.hostCounts, kCountWords * sizeof(uint32_t)));
+    if (!W.hostStats) CR_CUDA(cudaMallocHost(&W.hostStats, kStatWords * sizeof(unsigned long long)));
     cudaStream_t s = g.stream;
-    if (!g.gridTrace) {
-        g.gridTrace = occupancyGrid(reinterpret_cast<const void*>(k_trace<false>), 128, g.device);
-        g.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
-        g.gridShadeLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
-        g.gridShadeMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
-        g.gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen), 128, g.device);
+    if (!W.gridTrace) {
+        W.gridTrace = occupancyGrid(reinterpret_cast<const void*>(k_trace<false>), 128, g.device);
+        W.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
+        W.gridShadeLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
+        W.gridShadeMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
+        W.gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen), 128, g.device);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
-        g.gridSmall = sms * 8;
+        W.gridSmall = sms * 8;
+    }
+    if (tuning.env_alias && g.dev.env_has_image && !g.dev.alias_prob) {  // built on first request
+        crh::build_alias(g.env);
+        g.dev.alias_prob = g.aliasAlloc.upload(g.env.aliasProb.data(), g.env.aliasProb.size(), s);
+        g.dev.alias_index = g.aliasAlloc.upload(g.env.aliasIndex.data(), g.env.aliasIndex.size(), s);
     }
     CR_CUDA(cudaMemsetAsync(g.acc, 0, 3 * pixels * sizeof(double), s));
-    CR_CUDA(cudaMemsetAsync(g.stats, 0, kStatWords * sizeof(unsigned long long), s));
+    CR_CUDA(cudaMemsetAsync(W.stats, 0, kStatWords * sizeof(unsigned long long), s));
     const unsigned long long noError = ~0ull;
-    CR_CUDA(cudaMemcpyAsync(g.stats + kStatErrorKey, &noError, sizeof(noError), cudaMemcpyHostToDevice, s));
-    const ErrSink E{g.stats + kStatErrorKey, nullptr};
+    CR_CUDA(cudaMemcpyAsync(W.stats + kStatErrorKey, &noError, sizeof(noError), cudaMemcpyHostToDevice, s));
+    const ErrSink E{W.stats + kStatErrorKey, nullptr};
 
     const bool timePhases = tuning.time_phases != 0;
     double traceMs = 0, shadeMs = 0, regenMs = 0;
     uint64_t launches = 0;
     int iterations = 0, chunks = 0;
-    cudaEvent_t t0 = g.event(0), t1 = g.event(1);
+    cudaEvent_t t0 = W.event(0), t1 = W.event(1);
     CR_CUDA(cudaEventRecord(t0, s));
     auto lastProgress = start;
     bool errored = false;
@@ -970,10 +1019,10 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         const Chunk C{c0, std::min<uint64_t>(total, c0 + chunk), pixels};
         ++chunks;
         // the chunk's ids are issued from c0
-        CR_CUDA(cudaMemsetAsync(g.counts, 0, kCountWords * sizeof(uint32_t), s));
+        CR_CUDA(cudaMemsetAsync(W.counts, 0, kCountWords * sizeof(uint32_t), s));
         const unsigned long long issuedStart = c0;
-        CR_CUDA(cudaMemcpyAsync(g.stats + kStatIssued, &issuedStart, sizeof(issuedStart), cudaMemcpyHostToDevice, s));
-        k_pool_init<<<g.gridSmall, 128, 0, s>>>(g.q, static_cast<uint32_t>(pool));
+        CR_CUDA(cudaMemcpyAsync(W.stats + kStatIssued, &issuedStart, sizeof(issuedStart), cudaMemcpyHostToDevice, s));
+        k_pool_init<<<W.gridSmall, 128, 0, s>>>(W.q, static_cast<uint32_t>(pool));
         ++launches;
         const uint64_t maxIterations = ((C.c1 - C.c0) / pool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
         uint64_t iter = 0;
@@ -985,61 +1034,61 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
             ev = 2;
             for (int b = 0; b < batch; ++b) {
                 auto rec = [&](int phase, auto&& launch) {
-                    if (timePhases) CR_CUDA(cudaEventRecord(g.event(ev), s));
+                    if (timePhases) CR_CUDA(cudaEventRecord(W.event(ev), s));
                     launch();
-                    if (timePhases) { CR_CUDA(cudaEventRecord(g.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
+                    if (timePhases) { CR_CUDA(cudaEventRecord(W.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
                     ++launches;
                 };
-                rec(2, [&] { k_regen<<<g.gridRegen, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
+                rec(2, [&] { k_regen<<<W.gridRegen, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
                 rec(0, [&] {
-                    if (tuning.count_traversal) k_trace<true><<<g.gridTrace, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats);
-                    else k_trace<false><<<g.gridTrace, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats);
+                    if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats);
+                    else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats);
                 });
-                rec(1, [&] { k_shade<kShadeMiss><<<g.gridShadeMiss, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
-                rec(1, [&] { k_shade<kShadeNeeNull><<<g.gridShadeLight, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
-                rec(1, [&] { k_shade<kShadeGeneric><<<g.gridShade, 128, 0, s>>>(g.dev, P, g.st, g.q, cur, C, E, g.stats); });
+                rec(1, [&] { k_shade<kShadeMiss><<<W.gridShadeMiss, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
+                rec(1, [&] { k_shade<kShadeNeeNull><<<W.gridShadeLight, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
+                rec(1, [&] { k_shade<kShadeGeneric><<<W.gridShade, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
                 cur ^= 1;
                 ++iter;
                 ++iterations;
             }
-            CR_CUDA(cudaMemcpyAsync(g.hostCounts, g.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-            CR_CUDA(cudaMemcpyAsync(g.hostStats, g.stats, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaMemcpyAsync(W.hostCounts, W.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaMemcpyAsync(W.hostStats, W.stats, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
             CR_CUDA(cudaStreamSynchronize(s));
             CR_CUDA(cudaGetLastError());
             for (auto& te : timed) {
                 float ms = 0;
-                CR_CUDA(cudaEventElapsedTime(&ms, g.event(te.first), g.event(te.first + 1)));
+                CR_CUDA(cudaEventElapsedTime(&ms, W.event(te.first), W.event(te.first + 1)));
                 (te.second == 0 ? traceMs : te.second == 1 ? shadeMs : regenMs) += ms;
             }
             // after the last shade: live = next live queue + queued shadow rays
-            const uint64_t live = g.hostCounts[kCountExtend0 + cur] + g.hostCounts[kCountShadow0 + (cur ^ 1)];
-            const bool issuedAll = g.hostStats[kStatIssued] >= C.c1;
-            if (g.hostStats[kStatErrorKey] != ~0ull) { errored = true; break; }
+            const uint64_t live = W.hostCounts[kCountExtend0 + cur] + W.hostCounts[kCountShadow0 + (cur ^ 1)];
+            const bool issuedAll = W.hostStats[kStatIssued] >= C.c1;
+            if (W.hostStats[kStatErrorKey] != ~0ull) { errored = true; break; }
             if (issuedAll && live == 0) break;
             if (iter > maxIterations) throw crh::Error(CR_ERR_DEVICE_TIMEOUT, "paths still live after the iteration bound");
             if (progress) {
                 const auto now = std::chrono::steady_clock::now();
                 if (now - lastProgress >= std::chrono::seconds(2)) {
                     lastProgress = now;
-                    const uint64_t issued = std::min<uint64_t>(g.hostStats[kStatIssued], C.c1);
+                    const uint64_t issued = std::min<uint64_t>(W.hostStats[kStatIssued], C.c1);
                     const uint64_t done = issued > live ? issued - live : 0;
                     progress(done, total, std::chrono::duration<double>(now - start).count(), user);
                 }
             }
         }
         if (errored) break;
-        k_accumulate<<<g.gridSmall, 128, 0, s>>>(g.st.out, C, g.acc);
+        k_accumulate<<<W.gridSmall, 128, 0, s>>>(W.st.out, C, g.acc);
         ++launches;
         if (perSample) {
             const uint64_t n = C.c1 - C.c0;
-            k_pack_samples<<<g.gridSmall, 128, 0, s>>>(g.st.out, n, g.packed);
-            CR_CUDA(cudaMemcpyAsync(perSample + 3 * C.c0, g.packed, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+            k_pack_samples<<<W.gridSmall, 128, 0, s>>>(W.st.out, n, W.packed);
+            CR_CUDA(cudaMemcpyAsync(perSample + 3 * C.c0, W.packed, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
             CR_CUDA(cudaStreamSynchronize(s));
         }
     }
     if (errored) {
         // Re-run the first failing sample alone to recover the reference's message.
-        const unsigned long long key = g.hostStats[kStatErrorKey];
+        const unsigned long long key = W.hostStats[kStatErrorKey];
         const uint32_t sample = static_cast<uint32_t>(key & ((1ull << 21) - 1));
         const uint64_t rank = key >> 21;
         const uint64_t tilesX = (static_cast<uint64_t>(o.width) + 15) / 16;
@@ -1048,19 +1097,19 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         const uint32_t y = static_cast<uint32_t>((tile / tilesX) * 16 + within / 16);
         DevError host{};
         CR_CUDA(cudaStreamSynchronize(s));
-        CR_CUDA(cudaMemsetAsync(g.detail, 0, sizeof(DevError), s));
-        CR_CUDA(cudaMemsetAsync(g.stats, 0, 2 * sizeof(unsigned long long), s));
-        k_trace_one<<<1, 32, 0, s>>>(g.dev, P, g.st, y * static_cast<uint32_t>(o.width) + x, sample, g.detail, g.stats, g.stats + 1);
-        CR_CUDA(cudaMemcpyAsync(&host, g.detail, sizeof(DevError), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaMemsetAsync(W.detail, 0, sizeof(DevError), s));
+        CR_CUDA(cudaMemsetAsync(W.stats, 0, 2 * sizeof(unsigned long long), s));
+        k_trace_one<<<1, 32, 0, s>>>(g.dev, P, W.st, y * static_cast<uint32_t>(o.width) + x, sample, W.detail, W.stats, W.stats + 1);
+        CR_CUDA(cudaMemcpyAsync(&host, W.detail, sizeof(DevError), cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
         if (!host.code) { host.code = -1; host.x = static_cast<int32_t>(x); host.y = static_cast<int32_t>(y); host.sample = static_cast<int32_t>(sample); }
         throw crh::Error(CR_ERR_RENDER, crh::sample_error_message(host));
     }
-    k_film<<<g.gridSmall, 128, 0, s>>>(g.acc, g.film, pixels, o.samples);
+    k_film<<<W.gridSmall, 128, 0, s>>>(g.acc, g.film, pixels, o.samples);
     ++launches;
     CR_CUDA(cudaEventRecord(t1, s));
     if (filmHost) CR_CUDA(cudaMemcpyAsync(filmHost, g.film, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost, s));
-    CR_CUDA(cudaMemcpyAsync(g.hostStats, g.stats, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaMemcpyAsync(W.hostStats, W.stats, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaStreamSynchronize(s));
     CR_CUDA(cudaGetLastError());
     float deviceMs = 0;
@@ -1075,14 +1124,14 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         stats->chunks = chunks;
         stats->iterations = static_cast<uint64_t>(iterations);
         stats->camera_samples = total;
-        stats->boundary_retries = g.hostStats[kStatRetries];
-        stats->extend_rays = g.hostStats[kStatExtendRays];
-        stats->shadow_rays = g.hostStats[kStatShadowRays];
+        stats->boundary_retries = W.hostStats[kStatRetries];
+        stats->extend_rays = W.hostStats[kStatExtendRays];
+        stats->shadow_rays = W.hostStats[kStatShadowRays];
         stats->kernel_launches = launches;
-        stats->extend_pairs = g.hostStats[kStatPairs];
-        stats->extend_triangles = g.hostStats[kStatTris];
-        stats->shadow_pairs = g.hostStats[kStatShadowPairs];
-        stats->shadow_triangles = g.hostStats[kStatShadowTris];
+        stats->extend_pairs = W.hostStats[kStatPairs];
+        stats->extend_triangles = W.hostStats[kStatTris];
+        stats->shadow_pairs = W.hostStats[kStatShadowPairs];
+        stats->shadow_triangles = W.hostStats[kStatShadowTris];
     }
     if (progress) progress(total, total, seconds, user);
 }
@@ -1310,7 +1359,7 @@ cr_status cr_gpu_scene_destroy(cr_gpu_scene* scene) {
 
 cr_status cr_gpu_scene_bytes(const cr_gpu_scene* scene, uint64_t* bytes) {
     if (!scene || !bytes) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "scene or bytes is NULL");
-    *bytes = scene->geometry.bytes + scene->work.bytes + scene->filmAlloc.bytes + scene->outAlloc.bytes + scene->packedAlloc.bytes;
+    *bytes = scene->geometry.bytes + scene->aliasAlloc.bytes + scene->filmAlloc.bytes + workspaceFor(scene->device).bytes();
     return CR_OK;
 }
 

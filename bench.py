@@ -131,12 +131,12 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """DRAM bytes per closest-hit ray from the committed ncu summary (profiles/), if any."""
-    path = os.path.join(ROOT, "profiles", "extend_sphere_grid.json")
+    """DRAM bytes per traced ray (closest or any hit) of k_trace from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_trace_sphere_grid.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
-        return json.load(f).get("dram_bytes_per_extend_ray")
+        return json.load(f).get("dram_bytes_per_traced_ray")
 
 
 def cpu_reference_rate(sc, spp, threads):
@@ -272,18 +272,21 @@ def run_ours(args):
     }
 
     # end to end through the C ABI with host buffers: upload, render, download every step
-    e2e_secs, h2d = [], 0
+    # (K steps, each a new scene handle: create + render + film download + destroy)
+    e2e_secs = []
     film = None
-    for _ in range(2):
+    for _ in range(args.steps):
         barrier()
         t0 = time.perf_counter()
         ge = crgpu.GpuScene(tris, sc["materials"], env=env, bvh=(nodes, idx), device=local)
         film, _ = ge.render(cam, opt)
-        h2d = ge.bytes()
         ge.close()
         barrier()
         e2e_secs.append(time.perf_counter() - t0)
-    e2e_value = samples_per_step / min(e2e_secs) / 1e6 * world
+    t = torch.tensor([sum(e2e_secs)], dtype=torch.float64, device=device)
+    if distributed:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * samples_per_step * args.steps / float(t.item()) / 1e6
     h2d_bytes = int(tris.nbytes + nodes.nbytes + idx.nbytes + sc["env_image"].nbytes + sc["materials"].nbytes)
     d2h_bytes = int(film.nbytes)
 
@@ -307,7 +310,7 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
-                    "note": "scene upload + render + film download per step through cr_gpu_* with host arrays"},
+                    "note": "cr_gpu_scene_create (upload) + cr_gpu_render (film download) + destroy from host arrays, every one of K steps"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
         }

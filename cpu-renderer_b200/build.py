@@ -64,14 +64,17 @@ def build(force=False, verbose=False, ptxas_verbose=False, defines=(), out=None)
     inc = ["-I" + INCLUDE, "-I" + CSRC]
     tag = "" if out is None else "_" + os.path.basename(out).replace(".so", "")
     host_obj = os.path.join(BUILD, "cr_host.o")
-    dev_obj = os.path.join(BUILD, f"cr_render{tag}.o")
     _run(["g++"] + CXX_FLAGS + inc + ["-I/usr/local/cuda/include", "-c", os.path.join(CSRC, "cr_host.cpp"), "-o", host_obj], verbose)
     flags = NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-D" + d for d in defines]
-    r = _run([nvcc] + ARCH + flags + inc + ["-c", os.path.join(CSRC, "cr_render.cu"), "-o", dev_obj], verbose)
-    if ptxas_verbose:
-        sys.stderr.write(r.stdout + r.stderr)
+    dev_objs = []
+    for cu in sorted(f for f in os.listdir(CSRC) if f.endswith(".cu")):
+        obj = os.path.join(BUILD, cu[:-3] + tag + ".o")
+        r = _run([nvcc] + ARCH + flags + inc + ["-c", os.path.join(CSRC, cu), "-o", obj], verbose)
+        if ptxas_verbose:
+            sys.stderr.write(r.stdout + r.stderr)
+        dev_objs.append(obj)
     tmp = lib + ".tmp"
-    _run([nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", tmp, dev_obj, host_obj, "-lpthread"], verbose)
+    _run([nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", tmp] + dev_objs + [host_obj, "-lpthread"], verbose)
     os.replace(tmp, lib)
     return lib
 

@@ -115,7 +115,7 @@ class Stats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("exact_traversal", C.c_int32), ("env_alias", C.c_int32), ("paths_per_wave", C.c_int32),
-                ("block_size", C.c_int32), ("use_graphs", C.c_int32), ("time_phases", C.c_int32),
+                ("chunk_log2", C.c_int32), ("reserved", C.c_int32), ("time_phases", C.c_int32),
                 ("count_traversal", C.c_int32)]
 
 
@@ -143,6 +143,10 @@ def _ptr(a):
     return None if a is None or len(a) == 0 else a.ctypes.data
 
 
+ENCODE_SRGB8, ENCODE_RGBE, ENCODE_HDR_FILE = 0, 1, 2
+FRAME_FN = C.CFUNCTYPE(None, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p)
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError("libcr_b200.so is not built (run cpu-renderer_b200/build.py): " + LIB_PATH)
@@ -166,6 +170,11 @@ def _load():
         "cr_gpu_render_resident": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.POINTER(Stats), C.POINTER(Tuning), P]),
         "cr_gpu_film_download": (C.c_int, [P, P, C.c_uint64]),
         "cr_gpu_render_noalloc": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), P, C.POINTER(Stats)]),
+        "cr_display_thresholds": (C.c_int, [C.c_float, P]),
+        "cr_gpu_film_encode": (C.c_int, [P, C.c_int, C.c_float, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "cr_gpu_encode": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, P, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "cr_gpu_render_progressive": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.c_uint32, C.c_int, C.c_float,
+                                                FRAME_FN, P, P, C.POINTER(Stats), C.POINTER(Tuning)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -350,6 +359,45 @@ class GpuScene:
         out = np.zeros((height, width, 3), np.float32)
         check(lib.cr_gpu_film_download(self.handle, out.ctypes.data, out.size))
         return out
+
+    def film_encode(self, fmt=ENCODE_SRGB8, exposure=0.0):
+        """The last render's film encoded on the device (cr_gpu_film_encode): bytes."""
+        size = C.c_uint64(0)
+        check(lib.cr_gpu_film_encode(self.handle, fmt, exposure, None, 0, C.byref(size)))
+        out = np.zeros(size.value, np.uint8)
+        check(lib.cr_gpu_film_encode(self.handle, fmt, exposure, _ptr(out), size.value, C.byref(size)))
+        return out[:size.value].tobytes()
+
+    def render_progressive(self, camera, options, every, fmt=ENCODE_SRGB8, exposure=0.0, tuning=None):
+        """cr_gpu_render_progressive: returns ([(samples_done, frame bytes)], film, stats)."""
+        frames = []
+
+        def on_frame(done, data, size, user):
+            frames.append((done, C.string_at(data, size)))
+
+        cb = FRAME_FN(on_frame)
+        film = np.zeros((options.height, options.width, 3), np.float32)
+        stats = Stats()
+        check(lib.cr_gpu_render_progressive(self.handle, C.byref(camera), C.byref(options), every, fmt, exposure, cb, None,
+                                            film.ctypes.data, C.byref(stats), C.byref(tuning) if tuning else None))
+        return frames, film, stats.as_dict()
+
+
+def display_thresholds(exposure=0.0):
+    out = np.zeros(256, np.float32)
+    check(lib.cr_display_thresholds(exposure, out.ctypes.data))
+    return out
+
+
+def encode(film, fmt=ENCODE_SRGB8, exposure=0.0, device=0):
+    """A host film (H, W, 3) float32 encoded on the device (cr_gpu_encode): bytes."""
+    film = np.ascontiguousarray(film, dtype=np.float32)
+    h, w = film.shape[0], film.shape[1]
+    size = C.c_uint64(0)
+    check(lib.cr_gpu_encode(film.ctypes.data, w, h, fmt, exposure, device, None, 0, C.byref(size)))
+    out = np.zeros(max(1, size.value), np.uint8)
+    check(lib.cr_gpu_encode(film.ctypes.data, w, h, fmt, exposure, device, out.ctypes.data, size.value, C.byref(size)))
+    return out[:size.value].tobytes()
 
 
 def rel_mse(x, ref, eps=1e-2):

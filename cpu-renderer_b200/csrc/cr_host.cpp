@@ -566,6 +566,54 @@ std::string sample_error_message(const crg::DevError& e) {
     return "Pixel (" + std::to_string(e.x) + "," + std::to_string(e.y) + "), sample " + std::to_string(e.sample) + ": " + cause;
 }
 
+// ---- output encoding --------------------------------------------------------------------------
+
+void check_image_dims(int width, int height, const std::string& label) {
+    constexpr int maxDimension = 16384;
+    constexpr uint64_t maxPixels = 16777216;
+    if (width <= 0 || height <= 0 || width > maxDimension || height > maxDimension ||
+        static_cast<uint64_t>(width) > maxPixels / static_cast<uint64_t>(height))
+        throw Error(CR_ERR_INVALID_ARGUMENT,
+                    label + ": image dimensions must be positive, at most 16384 per axis and 16777216 pixels");
+}
+
+namespace {
+float linear_to_srgb(float v) {  // math.h:62
+    return v <= 0.0031308f ? 12.92f * v : 1.055f * std::pow(v, 1 / 2.4f) - 0.055f;
+}
+}  // namespace
+
+unsigned char display_channel(float value, double exposureScale) {  // image.cpp:119-124
+    const double x = static_cast<double>(value) * exposureScale;
+    const double filmic = std::clamp((x * (2.51 * x + 0.03)) / (x * (2.43 * x + 0.59) + 0.14), 0.0, 1.0);
+    const float srgb = linear_to_srgb(static_cast<float>(filmic));
+    return static_cast<unsigned char>(std::lround(std::clamp(srgb, 0.0f, 1.0f) * 255.0f));
+}
+
+void display_thresholds(float exposure, float out[256]) {
+    if (!std::isfinite(exposure) || exposure < -100 || exposure > 100)  // image.cpp:196-197
+        throw Error(CR_ERR_INVALID_ARGUMENT, "PNG exposure must be finite and between -100 and 100 stops");
+    const double scale = std::exp2(static_cast<double>(exposure));
+    constexpr uint32_t finiteEnd = 0x7f800000u;  // bit pattern of +inf; non-negative floats sort by bits
+    auto at = [&](uint32_t bits) { float f; std::memcpy(&f, &bits, 4); return display_channel(f, scale); };
+    const unsigned char top = at(finiteEnd - 1);
+    out[0] = 0.0f;
+    for (int k = 1; k < 256; ++k) {
+        if (top < k) { out[k] = std::numeric_limits<float>::infinity(); continue; }
+        uint32_t lo = 0, hi = finiteEnd - 1;  // invariant: at(hi) >= k
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (at(mid) >= k) hi = mid; else lo = mid + 1;
+        }
+        std::memcpy(&out[k], &hi, 4);
+    }
+}
+
+std::string hdr_header(int width, int height) {  // stb_image_write.h 1.16, stbi_write_hdr_core
+    return "#?RADIANCE\n# Written by stb_image_write.h\nFORMAT=32-bit_rle_rgbe\n"
+           "EXPOSURE=          1.0000000000000\n\n-Y " + std::to_string(height) + " +X " + std::to_string(width) + "\n";
+}
+
 }  // namespace crh
 
 // ---- C ABI entry points that need no GPU -------------------------------------------------------
@@ -642,6 +690,16 @@ cr_status cr_environment_tables(const cr_environment_desc* environment, double* 
         return CR_OK;
     } catch (const crh::Error& e) { return crh::set_last_error(e.status, e.what()); }
     catch (const std::bad_alloc&) { return crh::set_last_error(CR_ERR_OUT_OF_MEMORY, "host allocation failed"); }
+}
+
+cr_status cr_display_thresholds(float exposure, float* out256) {
+    try {
+        if (!out256) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        crh::display_thresholds(exposure, out256);
+        return CR_OK;
+    } catch (const crh::Error& e) {
+        return crh::set_last_error(e.status, e.what());
+    }
 }
 
 }  // extern "C"

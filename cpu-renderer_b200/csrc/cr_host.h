@@ -67,4 +67,18 @@ void camera_setup(const cr_camera& c, int width, int height, crg::DevCamera& out
 // Per-sample failure text, "Pixel (x,y), sample s: <cause>" (render.cpp:437-438).
 std::string sample_error_message(const crg::DevError& e);
 
+// ---- output encoding (src/io/image.cpp, src/io/file.h) -----------------------------------------
+// detail::imagePixels (file.h:84-89): positive, <= 16384 per axis, <= 16777216 pixels.
+void check_image_dims(int width, int height, const std::string& label);
+// The display mapping of io::writePng (image.cpp:116-124, 193-201) is a non-decreasing step
+// function of the linear value at a fixed exposure, so it is fully described by the least
+// value reaching each output byte: out[k] (k = 1..255) is the smallest non-negative float v
+// with displayChannel(v) >= k (+inf when none), out[0] = 0. Throws the reference's error for
+// an exposure outside [-100, 100] stops.
+void display_thresholds(float exposure, float out[256]);
+// The reference's display mapping itself, for checks of the table.
+unsigned char display_channel(float value, double exposure_scale);
+// The text stb_image_write 1.16 (the codec io::writeHdr uses) writes before the scanlines.
+std::string hdr_header(int width, int height);
+
 }  // namespace crh

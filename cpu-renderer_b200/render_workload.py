@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--time-phases", action="store_true")
     ap.add_argument("--count", action="store_true", help="count node pairs and triangles per closest-hit ray")
     ap.add_argument("--paths-per-wave", type=int, default=0)
+    ap.add_argument("--chunk-log2", type=int, default=0, help="2^n sample ids per chunk (0: automatic)")
     ap.add_argument("--out", help="write the film as .npy")
     a = ap.parse_args()
     t0 = time.time()
@@ -50,6 +51,7 @@ def main():
     tun.time_phases = int(a.time_phases)
     tun.count_traversal = int(a.count)
     tun.paths_per_wave = a.paths_per_wave
+    tun.chunk_log2 = a.chunk_log2
     for i in range(a.repeat):
         film, st = g.render(sc["camera"], opt, tuning=tun)
         st["msamples_per_s"] = st["camera_samples"] / st["device_ms"] / 1e3

@@ -223,8 +223,8 @@ typedef struct cr_gpu_tuning {
     int32_t exact_traversal;   /* 1: FP64 box tests in the reference's order for every ray */
     int32_t env_alias;         /* 1: alias-table environment sampling (different streams)   */
     int32_t paths_per_wave;    /* 0: automatic                                             */
-    int32_t block_size;        /* 0: automatic                                             */
-    int32_t use_graphs;        /* 0: automatic (on), -1: off                               */
+    int32_t chunk_log2;        /* 0: automatic; n in [16, 28]: 2^n sample ids per chunk     */
+    int32_t reserved;          /* must be 0                                                */
     int32_t time_phases;       /* 1: CUDA-event time every extend/shade/shadow launch      */
     int32_t count_traversal;   /* 1: count node pairs and triangles visited by closest-hit */
 } cr_gpu_tuning;
@@ -318,6 +318,55 @@ cr_status cr_gpu_film_download(cr_gpu_scene* scene, float* film_rgb, uint64_t fl
 cr_status cr_gpu_render_noalloc(cr_gpu_scene* scene, const cr_camera* camera,
                                 const cr_render_options* options, float* film_rgb,
                                 cr_render_stats* stats);
+
+/* ---- output encoding on the device ----------------------------------------------------------
+ * Replaces the per-pixel work of io::writePng / io::writeHdr (src/io/image.cpp:100-124,
+ * 193-230; scene.h:144-146), which the reference runs on the CPU after cr::render.
+ *   CR_ENCODE_SRGB8     width*height*3 bytes: exactly the 8-bit pixels io::writePng passes to
+ *                       its PNG codec (exposure in stops, filmic curve, sRGB, rounding).
+ *   CR_ENCODE_RGBE      width*height*4 bytes: the shared-exponent quads of the Radiance codec
+ *                       io::writeHdr uses (stb_image_write 1.16).
+ *   CR_ENCODE_HDR_FILE  the complete .hdr file io::writeHdr writes, byte for byte (header and
+ *                       run-length coded scanlines).
+ * Pixels are checked as the reference checks them (finite, non-negative; below 2^127 for the
+ * HDR forms; exposure within [-100, 100] for SRGB8) and fail with CR_ERR_INVALID_ARGUMENT and
+ * the reference's message. `*size` receives the encoded size. With out == NULL nothing is
+ * copied; with capacity below the size nothing is copied and CR_ERR_OUT_OF_RANGE returns. */
+typedef enum cr_encode_format {
+    CR_ENCODE_SRGB8 = 0,
+    CR_ENCODE_RGBE = 1,
+    CR_ENCODE_HDR_FILE = 2
+} cr_encode_format;
+
+/* Host-only. The table the SRGB8 encoder uses: out[k] (k = 1..255) is the least non-negative
+ * float whose display byte (io::writePng's mapping at `exposure` stops) is at least k, +inf
+ * when none is; out[0] = 0. The mapping is non-decreasing in the linear value, so a pixel's
+ * byte is the largest k with out[k] <= value. */
+cr_status cr_display_thresholds(float exposure, float* out256);
+
+/* Encodes the film of the scene's last cr_gpu_render / cr_gpu_render_resident /
+ * cr_gpu_render_progressive (the film cr_gpu_film_download returns) where it lies. */
+cr_status cr_gpu_film_encode(cr_gpu_scene* scene, int format, float exposure, void* out,
+                             uint64_t capacity, uint64_t* size);
+
+/* Encodes a caller's film (host memory, width*height*3 floats) on device `device`. */
+cr_status cr_gpu_encode(const float* film_rgb, int width, int height, int format, float exposure,
+                        int device, void* out, uint64_t capacity, uint64_t* size);
+
+/* Progressive output: cr::render's film after every `every_samples` samples per pixel.
+ * on_frame(samples_done, frame, size, user) is called on this thread with the encoded film
+ * (format and exposure as cr_gpu_film_encode) at samples_done = every_samples,
+ * 2*every_samples, ... and options->samples. Each frame is exactly the film a render with
+ * samples = samples_done would return (the per-pixel sums run in sample order). The frame
+ * buffer is valid during the call only. Requires every_samples*width*height <= 2^28.
+ * film_rgb and stats as cr_gpu_render (film_rgb may be NULL). No counterpart in the
+ * reference, whose render returns only the final film. */
+typedef void (*cr_frame_fn)(uint32_t samples_done, const void* frame, uint64_t size, void* user);
+cr_status cr_gpu_render_progressive(cr_gpu_scene* scene, const cr_camera* camera,
+                                    const cr_render_options* options, uint32_t every_samples,
+                                    int format, float exposure, cr_frame_fn on_frame, void* user,
+                                    float* film_rgb, cr_render_stats* stats,
+                                    const cr_gpu_tuning* tuning);
 
 #ifdef __cplusplus
 }

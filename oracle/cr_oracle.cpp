@@ -891,6 +891,81 @@ Scene makeScene(const cr_scene_desc* d, const cr_environment_desc* e, int brute)
     return S;
 }
 
+// ---- output encoding (src/io/image.cpp, src/io/file.h; stb_image_write 1.16) ---------------------
+// The checker for the device encoder: per-pixel direct evaluation of the reference's display
+// mapping, and the Radiance writer of the codec io::writeHdr calls, restated from its published
+// algorithm (third_party/stb_image_write.h: stbiw__linear_to_rgbe, stbiw__write_hdr_scanline,
+// stbi_write_hdr_core).
+
+void imagePixels(int width, int height, const std::string& label) {  // file.h:84-89
+    if (width <= 0 || height <= 0 || width > 16384 || height > 16384 ||
+        static_cast<std::size_t>(width) > 16777216u / static_cast<std::size_t>(height))
+        throw std::runtime_error(label + ": image dimensions must be positive, at most 16384 per axis and 16777216 pixels");
+}
+
+void validateOutput(int width, int height, const float* rgb, const std::string& label, bool hdr) {  // image.cpp:100-113
+    imagePixels(width, height, label);
+    const std::size_t n = static_cast<std::size_t>(width) * height;
+    for (std::size_t i = 0; i < n; ++i) {
+        const float r = rgb[3 * i], g = rgb[3 * i + 1], b = rgb[3 * i + 2];
+        if (!std::isfinite(r) || !std::isfinite(g) || !std::isfinite(b) || r < 0 || g < 0 || b < 0)
+            throw std::runtime_error(label + ": pixels must contain finite, nonnegative linear radiance");
+        if (hdr && std::max({r, g, b}) >= std::ldexp(1.0f, 127))
+            throw std::runtime_error(label + ": radiance exceeds the Radiance RGBE exponent range");
+    }
+}
+
+float linearToSrgb(float v) { return v <= 0.0031308f ? 12.92f * v : 1.055f * std::pow(v, 1 / 2.4f) - 0.055f; }  // math.h:62
+
+unsigned char displayChannel(float value, double exposureScale) {  // image.cpp:119-124
+    const double x = static_cast<double>(value) * exposureScale;
+    const double filmic = std::clamp((x * (2.51 * x + 0.03)) / (x * (2.43 * x + 0.59) + 0.14), 0.0, 1.0);
+    const float srgb = linearToSrgb(static_cast<float>(filmic));
+    return static_cast<unsigned char>(std::lround(std::clamp(srgb, 0.0f, 1.0f) * 255.0f));
+}
+
+void rgbe(const float* linear, unsigned char* out) {  // stbiw__linear_to_rgbe
+    const float m = std::max(linear[0], std::max(linear[1], linear[2]));
+    if (m < 1e-32f) { out[0] = out[1] = out[2] = out[3] = 0; return; }
+    int e;
+    const float normalize = static_cast<float>(std::frexp(m, &e)) * 256.0f / m;
+    for (int c = 0; c < 3; ++c) out[c] = static_cast<unsigned char>(static_cast<int>(linear[c] * normalize));
+    out[3] = static_cast<unsigned char>(e + 128);
+}
+
+// stbiw__write_hdr_scanline: run-length coding of each component of one scanline.
+void hdrScanline(const float* row, int width, std::vector<unsigned char>& out) {
+    std::vector<unsigned char> q(4 * static_cast<std::size_t>(width));
+    for (int x = 0; x < width; ++x) rgbe(row + 3 * x, &q[4 * x]);
+    if (width < 8 || width >= 32768) { out.insert(out.end(), q.begin(), q.end()); return; }
+    out.push_back(2); out.push_back(2);
+    out.push_back(static_cast<unsigned char>((width & 0xff00) >> 8)); out.push_back(static_cast<unsigned char>(width & 0xff));
+    for (int c = 0; c < 4; ++c) {
+        auto comp = [&](int x) { return q[4 * x + c]; };
+        int x = 0;
+        while (x < width) {
+            int r = x;  // start of the next run of three
+            while (r + 2 < width && !(comp(r) == comp(r + 1) && comp(r) == comp(r + 2))) ++r;
+            if (r + 2 >= width) r = width;
+            for (; x < r;) {  // literal pieces of at most 128
+                const int len = std::min(r - x, 128);
+                out.push_back(static_cast<unsigned char>(len));
+                for (int k = 0; k < len; ++k) out.push_back(comp(x + k));
+                x += len;
+            }
+            if (r + 2 < width) {  // the run, in pieces of at most 127
+                while (r < width && comp(r) == comp(x)) ++r;
+                for (; x < r;) {
+                    const int len = std::min(r - x, 127);
+                    out.push_back(static_cast<unsigned char>(len + 128));
+                    out.push_back(comp(x));
+                    x += len;
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 }  // namespace oracle
 
@@ -981,6 +1056,38 @@ int oracle_render(const cr_scene_desc* d, const cr_environment_desc* e, const cr
         if (retries) *retries = retry.load();
         return 0;
     } catch (const std::exception& ex) { lastError = ex.what(); return 2; }
+}
+
+// io::writePng's pixels (format 0), RGBE quads (1) or io::writeHdr's whole file (2).
+int oracle_encode(const float* rgb, int width, int height, int format, float exposure, unsigned char* out,
+                  uint64_t capacity, uint64_t* size) {
+    try {
+        std::vector<unsigned char> bytes;
+        if (format == 0) {
+            validateOutput(width, height, rgb, "PNG output", false);
+            if (!std::isfinite(exposure) || exposure < -100 || exposure > 100)
+                throw std::runtime_error("PNG exposure must be finite and between -100 and 100 stops");
+            const double scale = std::exp2(static_cast<double>(exposure));
+            const std::size_t n = 3 * static_cast<std::size_t>(width) * height;
+            bytes.resize(n);
+            for (std::size_t i = 0; i < n; ++i) bytes[i] = displayChannel(rgb[i], scale);
+        } else {
+            validateOutput(width, height, rgb, "HDR output", true);
+            if (format == 1) {
+                bytes.resize(4 * static_cast<std::size_t>(width) * height);
+                for (std::size_t i = 0; i < static_cast<std::size_t>(width) * height; ++i) rgbe(rgb + 3 * i, &bytes[4 * i]);
+            } else {
+                const std::string header = "#?RADIANCE\n# Written by stb_image_write.h\nFORMAT=32-bit_rle_rgbe\n"
+                                           "EXPOSURE=          1.0000000000000\n\n-Y " + std::to_string(height) +
+                                           " +X " + std::to_string(width) + "\n";
+                bytes.assign(header.begin(), header.end());
+                for (int y = 0; y < height; ++y) hdrScanline(rgb + 3 * static_cast<std::size_t>(y) * width, width, bytes);
+            }
+        }
+        *size = bytes.size();
+        if (out && capacity >= bytes.size()) std::memcpy(out, bytes.data(), bytes.size());
+        return 0;
+    } catch (const std::exception& ex) { lastError = ex.what(); return 1; }
 }
 
 }  // extern "C"

@@ -38,6 +38,8 @@ def lib():
         L.oracle_render.restype = C.c_int
         L.oracle_render.argtypes = [C.POINTER(SceneDesc), C.POINTER(EnvDesc), C.POINTER(Camera), C.POINTER(Options), C.c_int,
                                     P, P, C.POINTER(C.c_uint64)]
+        L.oracle_encode.restype = C.c_int
+        L.oracle_encode.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_float, P, C.c_uint64, C.POINTER(C.c_uint64)]
         _lib = L
     return _lib
 
@@ -123,3 +125,16 @@ def render(sc, options, threads=None):
     film, _, _ = render_arrays(tris, sc["materials"], bvh, sc["camera"], options, env=env, lights=sc.get("lights"),
                                images=sc.get("images", ()), textures=sc.get("textures"), threads=threads)
     return film
+
+
+def encode(film, fmt=0, exposure=0.0):
+    """io::writePng's pixels (fmt 0), RGBE quads (1) or io::writeHdr's file (2), restated."""
+    film = np.ascontiguousarray(film, dtype=np.float32)
+    h, w = (film.shape[0], film.shape[1]) if film.ndim == 3 else (0, 0)
+    size = C.c_uint64(0)
+    if lib().oracle_encode(film.ctypes.data, w, h, fmt, exposure, None, 0, C.byref(size)):
+        _err()
+    out = np.zeros(max(1, size.value), np.uint8)
+    if lib().oracle_encode(film.ctypes.data, w, h, fmt, exposure, out.ctypes.data, size.value, C.byref(size)):
+        _err()
+    return out[:size.value].tobytes()

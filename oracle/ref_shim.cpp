@@ -339,4 +339,22 @@ int ref_render(const void* s, const void* b, const cr_camera* c, const void* e, 
     } catch (const std::exception& e) { return fail(e); }
 }
 
+// ---- io::writePng / io::writeHdr (image.cpp:193-230), to files -----------------------------------
+int ref_write_png(const char* path, int width, int height, const float* rgb, float exposure) {
+    try {
+        std::vector<cr::Vec3> px(static_cast<size_t>(width > 0 && height > 0 ? width : 0) * static_cast<size_t>(height > 0 ? height : 0));
+        for (size_t i = 0; i < px.size(); ++i) px[i] = v3(rgb + 3 * i);
+        cr::io::writePng(path, width, height, px, exposure);
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+int ref_write_hdr(const char* path, int width, int height, const float* rgb) {
+    try {
+        std::vector<cr::Vec3> px(static_cast<size_t>(width > 0 && height > 0 ? width : 0) * static_cast<size_t>(height > 0 ? height : 0));
+        for (size_t i = 0; i < px.size(); ++i) px[i] = v3(rgb + 3 * i);
+        cr::io::writeHdr(path, width, height, px);
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
 }  // extern "C"

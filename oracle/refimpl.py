@@ -59,6 +59,8 @@ def lib():
             "ref_evaluate_bsdf": (None, [P, P, P, C.c_uint64, P]),
             "ref_options_validate": (C.c_int, [C.POINTER(Options)]),
             "ref_render": (C.c_int, [P, P, C.POINTER(Camera), P, C.POINTER(Options), P, C.POINTER(Stats)]),
+            "ref_write_png": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P, C.c_float]),
+            "ref_write_hdr": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -255,3 +257,21 @@ def validate_options(options):
     code = lib().ref_options_validate(C.byref(options))
     if code:
         _err(code)
+
+
+def write_png(path, film, exposure=0.0):
+    """io::writePng (image.cpp:193-212) of a (H, W, 3) float film."""
+    film = np.ascontiguousarray(film, dtype=np.float32)
+    h, w = (film.shape[0], film.shape[1]) if film.ndim == 3 else (0, 0)
+    rc = lib().ref_write_png(str(path).encode(), w, h, film.ctypes.data, exposure)
+    if rc:
+        _err(rc)
+
+
+def write_hdr(path, film):
+    """io::writeHdr (image.cpp:216-230) of a (H, W, 3) float film."""
+    film = np.ascontiguousarray(film, dtype=np.float32)
+    h, w = (film.shape[0], film.shape[1]) if film.ndim == 3 else (0, 0)
+    rc = lib().ref_write_hdr(str(path).encode(), w, h, film.ctypes.data)
+    if rc:
+        _err(rc)

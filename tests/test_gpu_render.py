@@ -119,10 +119,13 @@ def test_determinism_across_wave_sizes(crgpu, gpu):
     a, _ = g.render(cam, opt)
     b, _ = g.render(cam, opt)
     t = Tuning()
-    t.paths_per_wave = 5000  # a small pool: many iterations, samples finish far out of order
+    t.paths_per_wave = 5000  # a small pool: many chunks of 5000 samples
     c, st = g.render(cam, opt, tuning=t)
-    assert st["iterations"] > 100
-    assert a.tobytes() == b.tobytes() == c.tobytes()
+    assert st["iterations"] > 100 and st["chunks"] > 100
+    t.chunk_log2 = 18  # chunks of 2^18 samples through the 5000-slot pool: freed slots are refilled
+    d, st = g.render(cam, opt, tuning=t)
+    assert st["chunks"] == 4 and st["iterations"] > 100
+    assert a.tobytes() == b.tobytes() == c.tobytes() == d.tobytes()
 
 
 def test_film_is_the_ordered_double_sum_of_samples(crgpu, gpu):

@@ -66,13 +66,24 @@ def build(force=False, verbose=False, ptxas_verbose=False, defines=(), out=None)
     host_obj = os.path.join(BUILD, "cr_host.o")
     _run(["g++"] + CXX_FLAGS + inc + ["-I/usr/local/cuda/include", "-c", os.path.join(CSRC, "cr_host.cpp"), "-o", host_obj], verbose)
     flags = NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-D" + d for d in defines]
-    dev_objs = []
+    dev_objs, jobs = [], []
     for cu in sorted(f for f in os.listdir(CSRC) if f.endswith(".cu")):
         obj = os.path.join(BUILD, cu[:-3] + tag + ".o")
-        r = _run([nvcc] + ARCH + flags + inc + ["-c", os.path.join(CSRC, cu), "-o", obj], verbose)
-        if ptxas_verbose:
-            sys.stderr.write(r.stdout + r.stderr)
+        cmd = [nvcc] + ARCH + flags + inc + ["-c", os.path.join(CSRC, cu), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
         dev_objs.append(obj)
+    failed = None
+    for cmd, proc in jobs:  # the translation units compile in parallel
+        out, err = proc.communicate()
+        if proc.returncode != 0:
+            sys.stderr.write(out + err)
+            failed = cmd
+        elif ptxas_verbose or (verbose and (out or err)):
+            sys.stderr.write(out + err)
+    if failed:
+        raise RuntimeError("command failed: " + " ".join(failed))
     tmp = lib + ".tmp"
     _run([nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", tmp] + dev_objs + [host_obj, "-lpthread"], verbose)
     os.replace(tmp, lib)

@@ -147,6 +147,38 @@ ENCODE_SRGB8, ENCODE_RGBE, ENCODE_HDR_FILE = 0, 1, 2
 FRAME_FN = C.CFUNCTYPE(None, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p)
 
 
+class Job(C.Structure):
+    """cr_job: one render of a batch or server."""
+    _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("options", Options), ("film_rgb", C.c_void_p),
+                ("every_samples", C.c_uint32), ("format", C.c_int32), ("exposure", C.c_float), ("on_frame", FRAME_FN),
+                ("user", C.c_void_p), ("status", C.c_int), ("stats", Stats), ("submitted_at", C.c_double),
+                ("started_at", C.c_double), ("first_frame_at", C.c_double), ("finished_at", C.c_double),
+                ("error", C.c_char * 256)]
+
+
+class EngineTuning(C.Structure):
+    _fields_ = [("pool_paths", C.c_uint32), ("range_samples", C.c_uint32), ("refill_interval", C.c_uint32),
+                ("iterations_per_step", C.c_uint32), ("use_graphs", C.c_int32), ("reserved", C.c_int32),
+                ("memory_budget", C.c_uint64)]
+
+    @classmethod
+    def make(cls, pool_paths=0, range_samples=0, refill_interval=0, iterations_per_step=0, use_graphs=1, memory_budget=0):
+        return cls(pool_paths, range_samples, refill_interval, iterations_per_step, use_graphs, 0, memory_budget)
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class EngineStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("camera_samples", C.c_uint64), ("iterations", C.c_uint64),
+                ("launches", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("jobs_done", C.c_uint32), ("jobs_failed", C.c_uint32), ("peak_jobs", C.c_uint32),
+                ("graph_steps", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError("libcr_b200.so is not built (run cpu-renderer_b200/build.py): " + LIB_PATH)
@@ -175,6 +207,14 @@ def _load():
         "cr_gpu_encode": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, P, C.c_uint64, C.POINTER(C.c_uint64)]),
         "cr_gpu_render_progressive": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.c_uint32, C.c_int, C.c_float,
                                                 FRAME_FN, P, P, C.POINTER(Stats), C.POINTER(Tuning)]),
+        "cr_gpu_render_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning), C.POINTER(EngineStats)]),
+        "cr_gpu_autotune_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning)]),
+        "cr_server_create": (C.c_int, [C.c_int, C.POINTER(EngineTuning), C.POINTER(P)]),
+        "cr_server_submit": (C.c_int, [P, P, C.POINTER(C.c_uint64)]),
+        "cr_server_wait": (C.c_int, [P, C.c_uint64, C.c_double]),
+        "cr_server_stats": (C.c_int, [P, C.POINTER(EngineStats)]),
+        "cr_server_clock": (C.c_double, [P]),
+        "cr_server_destroy": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -412,3 +452,114 @@ def relative_l1(x, ref):
     x = np.asarray(x, np.float64)
     r = np.asarray(ref, np.float64)
     return float(np.abs(x - r).sum() / max(1e-12, r.sum()))
+
+
+class JobSpec:
+    """A render job: scene, camera, options, optional progressive frames. After the job ends,
+    .film (H, W, 3) float32 (when want_film), .frames [(samples_done, bytes)], .status,
+    .error, .stats and the engine-clock times are filled in."""
+
+    def __init__(self, scene, camera, options, every=0, fmt=ENCODE_SRGB8, exposure=0.0, want_film=True, keep_frames=True):
+        self.scene, self.camera, self.options = scene, camera, options
+        self.film = np.zeros((options.height, options.width, 3), np.float32) if want_film else None
+        self.frames = []
+        self.frame_times = []
+        self.job = Job()
+        j = self.job
+        j.scene = scene.handle
+        j.camera = camera
+        j.options = options
+        j.film_rgb = self.film.ctypes.data if want_film else None
+        j.every_samples = every
+        j.format = fmt
+        j.exposure = exposure
+        self._clock = None
+        keep = keep_frames
+
+        def on_frame(done, data, size, user):
+            self.frames.append((done, C.string_at(data, size) if keep else size))
+
+        self._cb = FRAME_FN(on_frame) if every else FRAME_FN(0)
+        j.on_frame = self._cb
+
+    @property
+    def status(self):
+        return self.job.status
+
+    @property
+    def error(self):
+        return self.job.error.decode()
+
+    @property
+    def stats(self):
+        return self.job.stats.as_dict()
+
+    @property
+    def times(self):
+        j = self.job
+        return {"submitted": j.submitted_at, "started": j.started_at, "first_frame": j.first_frame_at, "finished": j.finished_at}
+
+
+def render_batch(specs, tuning=None):
+    """cr_gpu_render_batch over JobSpecs; returns the engine stats (jobs report their own)."""
+    arr = (Job * len(specs))()
+    for i, sp in enumerate(specs):
+        arr[i] = sp.job
+    st = EngineStats()
+    status = lib.cr_gpu_render_batch(C.cast(arr, C.c_void_p), len(specs), C.byref(tuning) if tuning else None, C.byref(st))
+    for i, sp in enumerate(specs):
+        sp.job = arr[i]
+    if status != 0 and all(sp.job.status == 0 for sp in specs):  # an engine failure, not a job's
+        raise CrError(status, last_error())
+    return st.as_dict()
+
+
+def autotune_batch(specs, base=None):
+    arr = (Job * len(specs))()
+    for i, sp in enumerate(specs):
+        arr[i] = sp.job
+    t = base if base is not None else EngineTuning.make()
+    check(lib.cr_gpu_autotune_batch(C.cast(arr, C.c_void_p), len(specs), C.byref(t)))
+    return t
+
+
+class Server:
+    """cr_server: continuous batching on one device."""
+
+    def __init__(self, device=0, tuning=None):
+        h = C.c_void_p()
+        check(lib.cr_server_create(device, C.byref(tuning) if tuning else None, C.byref(h)))
+        self.handle = h
+        self._live = {}
+
+    def clock(self):
+        return lib.cr_server_clock(self.handle)
+
+    def submit(self, spec):
+        t = C.c_uint64(0)
+        check(lib.cr_server_submit(self.handle, C.byref(spec.job), C.byref(t)))
+        self._live[t.value] = spec
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        st = lib.cr_server_wait(self.handle, ticket, timeout)
+        if st != 7:
+            self._live.pop(ticket, None)
+        return st
+
+    def stats(self):
+        s = EngineStats()
+        check(lib.cr_server_stats(self.handle, C.byref(s)))
+        return s.as_dict()
+
+    def close(self):
+        if self.handle:
+            lib.cr_server_destroy(self.handle)
+            self.handle = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

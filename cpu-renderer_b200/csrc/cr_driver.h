@@ -1,0 +1,120 @@
+// Host-side pieces shared by the single-render driver (cr_render.cu) and the multi-job engine
+// (cr_engine.cu): CUDA error mapping, device allocations, the scene handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <exception>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cr_gpu.h"
+#include "cr_host.h"
+#include "cr_internal.h"
+
+namespace crd {
+
+struct CudaError : crh::Error {
+    CudaError(cudaError_t e, const char* what)
+        : crh::Error(e == cudaErrorMemoryAllocation ? CR_ERR_OUT_OF_MEMORY : CR_ERR_CUDA,
+                     std::string(what) + ": " + cudaGetErrorString(e)) {}
+};
+#define CR_CUDA(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) throw crd::CudaError(e_, #call); } while (0)
+
+// Device allocation owned by a scene.
+struct DevAlloc {
+    std::vector<void*> blocks;
+    uint64_t bytes = 0;
+    template <class T> T* alloc(size_t count) {
+        if (count == 0) count = 1;
+        void* p = nullptr;
+        CR_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        blocks.push_back(p);
+        bytes += count * sizeof(T);
+        return static_cast<T*>(p);
+    }
+    template <class T> T* upload(const T* src, size_t count, cudaStream_t s) {
+        T* d = alloc<T>(count);
+        if (count) CR_CUDA(cudaMemcpyAsync(d, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+        return d;
+    }
+    void release() {
+        for (void* p : blocks) cudaFree(p);
+        blocks.clear();
+        bytes = 0;
+    }
+};
+
+inline int occupancyGrid(const void* kernel, int block, int device) {
+    int sms = 0, perSm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, block, 0);
+    if (perSm < 1) perSm = 1;
+    return sms * perSm;
+}
+
+
+// The path pool's state arrays and queues for n slots.
+inline void allocPaths(DevAlloc& work, size_t n, crg::PathSoA& st, crg::Queues& q) {
+    using namespace crg;
+    st.ray_o = work.alloc<float4>(n); st.ray_d = work.alloc<float4>(n); st.ray_lo = work.alloc<float4>(n);
+    st.hit_tri = work.alloc<uint32_t>(n);
+    st.thr = work.alloc<float4>(n); st.rad = work.alloc<float4>(n); st.last_pos = work.alloc<float4>(n);
+    st.absorb = work.alloc<float4>(n); st.flags = work.alloc<uint32_t>(n);
+    st.rng = work.alloc<uint64_t>(n); st.prev_tri = work.alloc<uint32_t>(n);
+    st.pixel = work.alloc<uint32_t>(n); st.sample = work.alloc<uint32_t>(n); st.depth = work.alloc<uint32_t>(n);
+    st.sh_o = work.alloc<float4>(n); st.sh_d = work.alloc<float4>(n); st.sh_lo = work.alloc<float4>(n);
+    st.sh_c = work.alloc<float4>(n);
+    for (int k = 0; k < 2; ++k) {
+        q.extend[k] = work.alloc<uint32_t>(n);
+        q.shadow[k] = work.alloc<uint32_t>(n);
+        q.free[k] = work.alloc<uint32_t>(n);
+    }
+    for (int c = 0; c < kShadeClasses; ++c) q.shade[c] = work.alloc<uint32_t>(n);
+    q.counts = work.alloc<uint32_t>(kCountWords);
+}
+
+cr_status fail(const std::exception& e);
+cr_gpu_tuning defaults(const cr_gpu_tuning* t);
+crg::RenderParams makeParams(const cr_camera& camera, const cr_render_options& o, const cr_gpu_tuning& t);
+int referenceWorkers(const cr_render_options& o);
+
+}  // namespace crd
+
+struct cr_gpu_scene {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    crd::DevAlloc geometry;  // scene data
+    crg::DevScene dev{};
+    uint64_t triangleCount = 0;
+    crh::EnvTables env;  // host copy, for the alias table built on demand
+    crd::DevAlloc aliasAlloc;
+    // film of the last render: FP64 sums and the float film
+    double* acc = nullptr;
+    float* film = nullptr;
+    size_t filmPixels = 0;
+    int filmWidth = 0, filmHeight = 0;  // of the last render's film (0: none yet)
+    crd::DevAlloc filmAlloc;
+    std::mutex mutex;
+
+    ~cr_gpu_scene() {
+        if (device >= 0) cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        geometry.release();
+        aliasAlloc.release();
+        filmAlloc.release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void ensureFilm(size_t pixels) {
+        if (pixels <= filmPixels) return;
+        CR_CUDA(cudaStreamSynchronize(stream));
+        filmAlloc.release();
+        filmPixels = 0;
+        acc = filmAlloc.alloc<double>(3 * pixels);
+        film = filmAlloc.alloc<float>(3 * pixels);
+        filmPixels = pixels;
+    }
+};
+

@@ -1,0 +1,654 @@
+// Device code of the path tracer: per-path functions (camera sample, closest/any hit, one
+// bounce of trace()) and the kernels that run them over the path pool. Included by the
+// single-render driver (cr_render.cu) and the multi-job engine (cr_engine.cu); kernels that
+// both use are templates or static, so each translation unit holds its own instantiation.
+#pragma once
+#include "cr_shade.cuh"
+
+// Minimum resident blocks per SM requested from the register allocator (128-thread blocks).
+// k_trace at 12 (40 registers, some spills to L1) measured ~2 % faster than at 8 or 10 on
+// the 1M-triangle workload; k_shade above 4 loses more to spills than it gains.
+#ifndef CR_TRACE_MIN_BLOCKS
+#define CR_TRACE_MIN_BLOCKS 12
+#endif
+#ifndef CR_SHADE_MIN_BLOCKS
+#define CR_SHADE_MIN_BLOCKS 4
+#endif
+
+namespace crg {
+
+// A chunk of consecutive sample ids [c0, c1); out[] holds their radiance at id - c0.
+struct Chunk {
+    uint64_t c0, c1, pixels;
+};
+
+// Where a path's sample radiance goes: out[base + sample * pixels + pixel].
+struct OutRef {
+    uint64_t base, pixels;
+};
+CR_D OutRef outOf(const Chunk& C) { return OutRef{0ull - C.c0, C.pixels}; }
+
+// ---- multi-job pool ----------------------------------------------------------------------------
+// In the multi-job engine the paths of many renders (jobs: scene, camera, options) share one
+// pool. The host appends sample ranges of its jobs to an issue list; free slots take the next
+// positions of the list. Each path remembers its range, which names its job's scene and
+// parameters, where its radiance goes, and the counter of finished samples the host polls.
+struct IssueRange {
+    uint64_t start;    // position of the range's first sample in the issue list
+    uint64_t c0, c1;   // the job's sample ids [c0, c1), numbered as in a single render
+    uint64_t outBase;  // out[] index of sample id c0
+    uint64_t pixels;   // the job's width * height
+    uint32_t job;      // job slot
+    uint32_t pad;
+};
+struct JobTable {
+    const DevScene* scenes;          // [job slot]
+    const RenderParams* params;      // [job slot]
+    const IssueRange* ranges;        // the issue list
+    const unsigned long long* ctl;   // [0] issue end: positions below it may start; [1] range count
+    unsigned long long* issued;      // [2] next issue position, ping-pong by iteration parity
+    unsigned long long* done;        // [range] finished samples
+    unsigned long long* errKeys;     // [job slot] smallest error key
+    unsigned long long* retries;     // [job slot] precision replays
+    uint32_t* range;                 // [path slot] the path's range
+};
+
+enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatPairs = 4, kStatTris = 5,
+       kStatIssued = 6, kStatShadowPairs = 7, kStatShadowTris = 8, kStatWords = 12 };
+
+CR_D uint64_t errorKey(const RenderParams& P, uint32_t pixel, uint32_t sample) {
+    const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
+    const uint64_t tilesX = (static_cast<uint64_t>(P.width) + 15) / 16;
+    const uint64_t rank = ((y / 16) * tilesX + x / 16) * 256 + (y % 16) * 16 + (x % 16);
+    return (rank << 21) | sample;
+}
+
+// Error sink: the smallest key is kept for the report; when detail is set (single-sample
+// re-run), the full record is written there.
+struct ErrSink {
+    unsigned long long* minKey;
+    DevError* detail;
+};
+CR_D void raise(const ErrSink& E, const RenderParams& P, uint32_t pixel, uint32_t sample, int code) {
+    atomicMin(E.minKey, static_cast<unsigned long long>(errorKey(P, pixel, sample)));
+    if (E.detail) {
+        E.detail->code = code;
+        E.detail->x = static_cast<int32_t>(pixel % static_cast<uint32_t>(P.width));
+        E.detail->y = static_cast<int32_t>(pixel / static_cast<uint32_t>(P.width));
+        E.detail->sample = static_cast<int32_t>(sample);
+        E.detail->key = errorKey(P, pixel, sample);
+    }
+}
+
+// All 32 lanes call this together; lanes with pred append value to the queue.
+CR_D void warpPush(uint32_t* queue, uint32_t* counter, bool pred, uint32_t value) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) queue[base + __popc(mask & ((1u << lane) - 1u))] = value;
+}
+
+CR_D float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// render.cpp:396-401 plus trace()'s initial state (render.cpp:235-239).
+CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t slot, uint32_t pixel,
+                   uint32_t sample, bool precise, const ErrSink& E) {
+    Rng rng(sampleSeed(P.seed, pixel, sample));
+    const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
+    const float dx = rng.uniform(), dy = rng.uniform();
+    TRay ray;
+    if (!cameraRay(P.camera, P.width, P.height, static_cast<float>(x) + dx, static_cast<float>(y) + dy, ray)) {
+        raise(E, P, pixel, sample, kErrUnrepresentableCameraRay);
+        return false;
+    }
+    st.ray_o[slot] = f4(ray.o, ray.tmin);
+    st.ray_d[slot] = f4(ray.d, ray.tmax);
+    st.ray_lo[slot] = make_float4(0, 0, 0, 0);
+    st.thr[slot] = make_float4(1, 1, 1, 1);          // throughput 1, etaScale 1
+    st.rad[slot] = make_float4(0, 0, 0, 0);          // radiance 0, lastPdf 0
+    st.last_pos[slot] = make_float4(0, 0, 0, 0);
+    st.absorb[slot] = make_float4(0, 0, 0, __int_as_float(-1));  // medium -1
+    st.flags[slot] = kPathLastDelta | (precise ? kPathPrecise : 0u);
+    st.rng[slot] = rng.state;
+    st.prev_tri[slot] = kNoTriangle;
+    st.pixel[slot] = pixel;
+    st.sample[slot] = sample;
+    st.depth[slot] = 0;
+    return true;
+}
+
+CR_D TRay loadRay(const PathSoA& st, uint32_t path, uint32_t flags) {
+    const float4 o = st.ray_o[path], d = st.ray_d[path];
+    TRay r;
+    r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w;
+    r.olow = (flags & kPathPrecise) ? v3(st.ray_lo[path]) : V3{};
+    return r;
+}
+
+// Ends a path: the reference's final radiance check (render.cpp:346), then the sample output.
+CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path, V3 R, const ErrSink& E) {
+    const uint32_t pixel = st.pixel[path], sample = st.sample[path];
+    if (!finite3(R) || smin3(R.x, R.y, R.z) < 0) {
+        raise(E, P, pixel, sample, kErrNonFiniteRadiance);
+        R = V3{};
+    }
+    st.out[O.base + static_cast<uint64_t>(sample) * O.pixels + pixel] = f4(R, 0);
+}
+
+// One iteration of trace()'s bounce loop (render.cpp:240-344) for one path, after its
+// closest hit is known. cont: the path continues; shadow: a shadow ray was queued (a path
+// that ends with a queued shadow ray is finished by k_trace next iteration); freed: the path
+// ended and its slot can take a new sample. CLASS specialises the code: kShadeMiss holds only
+// environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeGeneric anything.
+template <int CLASS>
+CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
+                   const ErrSink& E, unsigned long long* retries, bool& cont, bool& shadow, bool& freed) {
+    cont = false; shadow = false; freed = false;
+    uint32_t flags = st.flags[path];
+    const bool precise = flags & kPathPrecise;
+    const TRay ray = loadRay(st, path, flags);
+    const float4 th = st.thr[path], ra = st.rad[path], ab = st.absorb[path];
+    V3 T = v3(th), R = v3(ra), A = v3(ab);
+    float etaScale = th.w, lastPdf = ra.w;
+    int medium = __float_as_int(ab.w);
+    bool lastDelta = flags & kPathLastDelta;
+    const V3 lastPosition = v3(st.last_pos[path]);
+    const uint32_t depth = st.depth[path];
+    const uint32_t pixel = st.pixel[path], sample = st.sample[path];
+    Rng rng(st.rng[path]);
+    const uint32_t tri = st.hit_tri[path];
+    int err = 0;
+    auto finish = [&](V3 radiance) { finishPath(P, O, st, path, radiance, E); freed = true; };
+
+    if (CLASS == kShadeMiss || (CLASS == kShadeGeneric && tri == kNoTriangle)) {  // render.cpp:242-248
+        if (medium >= 0) T = T * beerLambert(A, kInf);
+        const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, environmentPdf(S, ray.d));
+        R = R + T * envRadiance(S, ray.d) * weight;
+        finish(R);
+        return;
+    }
+    // The traversal reported the triangle; t, u and v come from the same FP64 arithmetic.
+    const cr_triangle& tr = S.tris[tri];
+    const ExactSetup X = exact_setup(ray);
+    double t = 0, w1 = 0, w2 = 0, det = 1;
+    tri_exact(X, v3(tr.v[0].position), v3(tr.v[1].position), v3(tr.v[2].position), -static_cast<double>(kInf),
+              static_cast<double>(kInf), t, w1, w2, det);
+    const double hu = w1 / det, hv = w2 / det;
+    if (medium >= 0) T = T * beerLambert(A, static_cast<float>(t));
+    const Surface s = surfaceAt(S, ray.d, tri, hu, hv, err);
+    if (s.frontFace || s.doubleSided) {
+        const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, trianglePdf(S, tri, lastPosition, s.position));
+        R = R + T * s.emission * weight;
+    }
+    if (static_cast<int>(depth) == P.bounces) {
+        if (err) { raise(E, P, pixel, sample, err); }
+        finish(R);
+        return;
+    }
+    const V3 wo = -ray.d;
+    bool pending = false;
+    TRay sh;
+    V3 contrib;
+    if (CLASS == kShadeNeeNull && P.nee) {
+        skipLight(S, rng, P.env_alias != 0);  // zero BSDF: the sample cannot contribute
+    } else if (P.nee) {  // render.cpp:262-299
+        const LightSample light = sampleLight(S, s.position, rng, P.env_alias, err);
+        const bool enclosedInfinite = medium >= 0 && s.thickness <= 0 && !isfin(light.distance);
+        if (!enclosedInfinite && light.pdf > 0 && maxComponent(light.radiance) > 0) {
+            const BsdfEval bsdf = evaluateBsdf(s, wo, light.direction);
+            if (maxComponent(bsdf.value) > 0) {
+                bool ok = true;
+                if (precise) { sh.o = s.position; sh.d = light.direction; sh.tmin = 0; sh.tmax = kInf; sh.olow = s.positionLow; }
+                else ok = offsetRay(s.position, s.geometricNormal, light.direction, kInf, sh, err);
+                if (ok && isfin(light.distance)) {
+                    V3 end = light.target;
+                    if (lengthSquared(light.targetNormal) > 0) {
+                        TRay moved;
+                        ok = offsetRay(end, light.targetNormal, -light.direction, kInf, moved, err);
+                        end = moved.o;
+                    }
+                    const V3 delta = end - sh.o;
+                    sh.tmax = length(delta) * (1 - 2e-6f);
+                    sh.d = normalize(delta);
+                }
+                if (ok) {
+                    const float weight = light.delta ? 1 : powerHeuristic(light.pdf, bsdf.pdf);
+                    V3 shadowAbsorption = A;
+                    bool shadowInMedium = medium >= 0;
+                    if (s.thickness > 0 && dot(wo, s.geometricNormal) * dot(light.direction, s.geometricNormal) < 0) {
+                        shadowInMedium = s.frontFace;
+                        shadowAbsorption = s.frontFace ? absorptionCoefficient(s.attenuationColor, s.attenuationDistance) : V3{};
+                    }
+                    const V3 transmittance = shadowInMedium ? beerLambert(shadowAbsorption, light.distance) : V3{1};
+                    contrib = T * bsdf.value * light.radiance * transmittance *
+                              (fabsf(dot(s.normal, light.direction)) * weight / light.pdf);
+                    pending = true;
+                }
+            }
+        }
+    }
+    if (err) {  // an exception inside trace(): the sample fails
+        raise(E, P, pixel, sample, err);
+        finish(V3{});
+        return;
+    }
+    const uint32_t ignore = precise ? tri : kNoTriangle;
+    auto queueShadow = [&](bool dead) {
+        st.sh_o[path] = f4(sh.o, sh.tmin);
+        st.sh_d[path] = f4(sh.d, sh.tmax);
+        st.sh_lo[path] = f4(sh.olow, __uint_as_float(ignore));
+        st.sh_c[path] = f4(contrib, 0);
+        shadow = true;
+        if (dead) {
+            st.rad[path] = f4(R, lastPdf);
+            st.flags[path] = flags | kPathDead | kPathShadow;
+        }
+    };
+    const BsdfSample smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
+    if (!smp.ok()) {
+        if (pending) queueShadow(true); else finish(R);
+        return;
+    }
+    T = T * smp.weight;
+    if (!finite3(T)) {
+        raise(E, P, pixel, sample, kErrNonFiniteThroughput);
+        finish(V3{});
+        return;
+    }
+    int boundary = 0;
+    if (smp.transmitted && s.thickness > 0) {  // render.cpp:306-329
+        if (s.frontFace) {
+            if (medium >= 0) boundary = kErrNestedVolume;
+            else { medium = static_cast<int>(s.material); A = absorptionCoefficient(s.attenuationColor, s.attenuationDistance); }
+        } else {
+            if (medium < 0) boundary = kErrExitWithoutEntry;
+            else { medium = -1; A = V3{}; }
+        }
+        if (!boundary) etaScale *= smp.eta * smp.eta;
+    }
+    if (boundary) {
+        if (!precise) {  // render.cpp:404-411: replay the same sample from split origins
+            atomicAdd(retries, 1ull);
+            initPath(S, P, st, path, pixel, sample, true, E);
+            cont = true;
+            return;
+        }
+        raise(E, P, pixel, sample, boundary);
+        if (E.detail && boundary == kErrExitWithoutEntry) {
+            E.detail->depth = static_cast<int32_t>(depth);
+            E.detail->triangle = tri;
+            E.detail->material = s.material;
+            E.detail->t = t;
+            E.detail->point[0] = s.position.x; E.detail->point[1] = s.position.y; E.detail->point[2] = s.position.z;
+            E.detail->origin[0] = ray.o.x; E.detail->origin[1] = ray.o.y; E.detail->origin[2] = ray.o.z;
+            E.detail->direction[0] = ray.d.x; E.detail->direction[1] = ray.d.y; E.detail->direction[2] = ray.d.z;
+        }
+        finish(V3{});
+        return;
+    }
+    lastPdf = smp.pdf;
+    lastDelta = smp.delta;
+    TRay next;
+    if (precise) { next.o = s.position; next.d = smp.direction; next.tmin = 0; next.tmax = kInf; next.olow = s.positionLow; }
+    else if (!offsetRay(s.position, s.geometricNormal, smp.direction, kInf, next, err)) {
+        raise(E, P, pixel, sample, err);
+        finish(V3{});
+        return;
+    }
+    if (P.rr && depth >= 3) {  // render.cpp:337-343
+        const float survive = sclamp(maxComponent(T) * etaScale, 0.05f, 0.95f);
+        if (rng.uniform() >= survive) {
+            if (pending) queueShadow(true); else finish(R);
+            return;
+        }
+        T = T * (1 / survive);
+    }
+    // continue
+    st.ray_o[path] = f4(next.o, next.tmin);
+    st.ray_d[path] = f4(next.d, next.tmax);
+    if (precise) st.ray_lo[path] = f4(next.olow, 0);
+    st.thr[path] = f4(T, etaScale);
+    st.rad[path] = f4(R, lastPdf);
+    st.last_pos[path] = f4(s.position, 0);
+    st.absorb[path] = f4(A, __int_as_float(medium));
+    flags = (flags & kPathPrecise) | (lastDelta ? kPathLastDelta : 0u);
+    st.flags[path] = flags;
+    st.rng[path] = rng.state;
+    st.prev_tri[path] = ignore;
+    st.depth[path] = depth + 1;
+    if (pending) queueShadow(false);
+    cont = true;
+}
+
+// Any hit for one queued shadow ray; an unoccluded contribution is added (render.cpp:283-296).
+// Returns true when the path had ended and its slot is now free.
+template <bool COUNT = false>
+CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
+                    const ErrSink& E, unsigned long long* stats = nullptr) {
+    const float4 o = st.sh_o[path], d = st.sh_d[path], lo = st.sh_lo[path], c = st.sh_c[path];
+    TRay r;
+    r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w; r.olow = v3(lo);
+    HitRec h;
+    h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
+    int err = 0;
+    VisitCount vc;
+    const bool blocked = intersect<true, COUNT>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0,
+                                                h, err, &vc);
+    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    if (COUNT) {
+        atomicAdd(&stats[kStatShadowPairs], static_cast<unsigned long long>(vc.pairs));
+        atomicAdd(&stats[kStatShadowTris], static_cast<unsigned long long>(vc.tris));
+    }
+    const float4 ra = st.rad[path];
+    V3 R = v3(ra);
+    if (!blocked) R = R + v3(c);
+    const uint32_t flags = st.flags[path];
+    if (flags & kPathDead) { finishPath(P, O, st, path, R, E); return true; }
+    st.rad[path] = f4(R, ra.w);
+    return false;
+}
+
+template <bool COUNT>
+CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
+                    unsigned long long* stats) {
+    const uint32_t flags = st.flags[path];
+    const TRay r = loadRay(st, path, flags);
+    HitRec h;
+    h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
+    int err = 0;
+    VisitCount vc;
+    const bool found = intersect<false, COUNT>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
+                                               h, err, &vc);
+    st.hit_tri[path] = found ? h.tri : kNoTriangle;
+    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    if (COUNT) {
+        atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
+        atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
+    }
+    if (!found) return kShadeMiss;
+    return (S.nee_skip && (h.flags & kTriNeeNull)) ? kShadeNeeNull : kShadeGeneric;
+}
+
+// The job of a path in the multi-job pool.
+struct PathJob {
+    const DevScene* S;
+    const RenderParams* P;
+    OutRef O;
+    ErrSink E;
+    unsigned long long* retries;
+    uint32_t r;
+};
+CR_D PathJob pathJob(const JobTable& J, uint32_t path) {
+    const uint32_t r = J.range[path];
+    const IssueRange& R = J.ranges[r];
+    PathJob pj;
+    pj.S = J.scenes + R.job;
+    pj.P = J.params + R.job;
+    pj.O = OutRef{R.outBase - R.c0, R.pixels};
+    pj.E = ErrSink{J.errKeys + R.job, nullptr};
+    pj.retries = J.retries + R.job;
+    pj.r = r;
+    return pj;
+}
+// The range holding issue position pos (the last range starting at or before it).
+CR_D uint32_t findRange(const JobTable& J, uint32_t count, uint64_t pos) {
+    uint32_t lo = 0, hi = count;  // ranges[lo].start <= pos < ranges[hi].start
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (J.ranges[mid].start <= pos) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+// All 32 lanes call this together: lanes whose sample finished count it in its range, one
+// atomic per distinct range among them.
+CR_D void countDone(const JobTable& J, bool finished, uint32_t r) {
+    const unsigned active = __ballot_sync(0xffffffffu, finished);
+    if (!finished) return;
+    const unsigned peers = __match_any_sync(active, r);
+    if (static_cast<int>(threadIdx.x & 31) == __ffs(peers) - 1)
+        atomicAdd(&J.done[r], static_cast<unsigned long long>(__popc(peers)));
+}
+
+// ---- kernels -----------------------------------------------------------------------------------
+// Every pool slot starts free (in free[1], which the first k_regen reads).
+static __global__ void k_pool_init(Queues q, uint32_t pool) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pool; i += gridDim.x * blockDim.x) q.free[1][i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) q.counts[kCountFree1] = pool;
+}
+
+// Free slots take the next sample ids of the chunk, in order (single render), or the next
+// positions of the issue list (MULTI: only when `refill`, and only up to the host's issue end;
+// slots left without work stay in the free queue).
+template <bool MULTI>
+__global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+                                               unsigned long long* stats, JobTable J, int refill) {
+    const uint32_t n = q.counts[kCountFree0 + (cur ^ 1)];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        q.counts[kCountFree0 + cur] = 0;
+        for (int c = 0; c < kShadeClasses; ++c) q.counts[kCountShade0 + c] = 0;
+    }
+    const uint32_t* freeQ = q.free[cur ^ 1];
+    if constexpr (!MULTI) {
+        for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+            const uint32_t idx = base + threadIdx.x;
+            const bool have = idx < n;
+            const uint32_t slot = have ? freeQ[idx] : 0;
+            const unsigned mask = __ballot_sync(0xffffffffu, have);
+            const int lane = threadIdx.x & 31;
+            unsigned long long first = 0;
+            if (mask) {
+                const int leader = __ffs(mask) - 1;
+                if (lane == leader) first = atomicAdd(&stats[kStatIssued], static_cast<unsigned long long>(__popc(mask)));
+                first = __shfl_sync(0xffffffffu, first, leader);
+            }
+            const uint64_t id = first + __popc(mask & ((1u << lane) - 1u));
+            bool live = false;
+            if (have && id < C.c1) {
+                const uint32_t pixel = static_cast<uint32_t>(id % C.pixels), sample = static_cast<uint32_t>(id / C.pixels);
+                live = initPath(S, P, st, slot, pixel, sample, false, E);
+                if (!live) st.out[id - C.c0] = make_float4(0, 0, 0, 0);
+            }
+            warpPush(q.extend[cur], &q.counts[kCountExtend0 + cur], live, slot);
+        }
+    } else {
+        const unsigned long long first = J.issued[cur ^ 1];
+        const unsigned long long end = J.ctl[0];
+        const uint32_t rangeCount = static_cast<uint32_t>(J.ctl[1]);
+        const uint64_t avail = end > first ? end - first : 0;
+        const uint32_t claimed = refill ? static_cast<uint32_t>(avail < n ? avail : n) : 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) J.issued[cur] = first + claimed;
+        for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+            const uint32_t idx = base + threadIdx.x;
+            const bool have = idx < n;
+            const uint32_t slot = have ? freeQ[idx] : 0;
+            bool live = false, keep = false, failed = false;
+            uint32_t r = 0;
+            if (have && idx < claimed) {
+                const uint64_t pos = first + idx;
+                r = findRange(J, rangeCount, pos);
+                const IssueRange& R = J.ranges[r];
+                const uint64_t id = R.c0 + (pos - R.start);
+                const uint32_t pixel = static_cast<uint32_t>(id % R.pixels), sample = static_cast<uint32_t>(id / R.pixels);
+                J.range[slot] = r;
+                const ErrSink Ej{J.errKeys + R.job, nullptr};
+                live = initPath(J.scenes[R.job], J.params[R.job], st, slot, pixel, sample, false, Ej);
+                if (!live) {
+                    st.out[R.outBase + (id - R.c0)] = make_float4(0, 0, 0, 0);
+                    failed = keep = true;
+                }
+            } else if (have) {
+                keep = true;
+            }
+            warpPush(q.extend[cur], &q.counts[kCountExtend0 + cur], live, slot);
+            warpPush(q.free[cur], &q.counts[kCountFree0 + cur], keep, slot);
+            countDone(J, failed, r);
+        }
+    }
+}
+
+// Closest hit for the live queue and any hit for last iteration's shadow rays, one launch.
+template <bool COUNT, bool MULTI = false>
+__global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+                                               unsigned long long* stats, JobTable J) {
+    const uint32_t nE = q.counts[kCountExtend0 + cur];
+    const uint32_t nS = q.counts[kCountShadow0 + (cur ^ 1)];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        q.counts[kCountExtend0 + (cur ^ 1)] = 0;
+        q.counts[kCountShadow0 + cur] = 0;
+        stats[kStatExtendRays] += nE;
+        stats[kStatShadowRays] += nS;
+    }
+    const uint32_t total = nE + nS;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        bool freed = false;
+        int cls = -1;
+        uint32_t path = 0, r = 0;
+        if (idx < nE) {
+            path = q.extend[cur][idx];
+            if constexpr (MULTI) {
+                const PathJob pj = pathJob(J, path);
+                cls = closestOne<COUNT>(*pj.S, *pj.P, st, path, pj.E, stats);
+            } else {
+                cls = closestOne<COUNT>(S, P, st, path, E, stats);
+            }
+        } else if (idx < total) {
+            path = q.shadow[cur ^ 1][idx - nE];
+            if constexpr (MULTI) {
+                const PathJob pj = pathJob(J, path);
+                freed = shadowOne<COUNT>(*pj.S, *pj.P, pj.O, st, path, pj.E, stats);
+                r = pj.r;
+            } else {
+                freed = shadowOne<COUNT>(S, P, outOf(C), st, path, E, stats);
+            }
+        }
+        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
+        if constexpr (MULTI) countDone(J, freed, r);
+#pragma unroll
+        for (int c = 0; c < kShadeClasses; ++c) warpPush(q.shade[c], &q.counts[kCountShade0 + c], cls == c, path);
+    }
+}
+
+template <int CLASS, bool MULTI = false>
+__global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+                                               unsigned long long* stats, JobTable J) {
+    const uint32_t n = q.counts[kCountShade0 + CLASS];
+    const uint32_t* in = q.shade[CLASS];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t idx = base + threadIdx.x;
+        bool cont = false, shadow = false, freed = false;
+        uint32_t path = 0, r = 0;
+        if (idx < n) {
+            path = in[idx];
+            if constexpr (MULTI) {
+                const PathJob pj = pathJob(J, path);
+                shadeOne<CLASS>(*pj.S, *pj.P, pj.O, st, path, pj.E, pj.retries, cont, shadow, freed);
+                r = pj.r;
+            } else {
+                shadeOne<CLASS>(S, P, outOf(C), st, path, E, &stats[kStatRetries], cont, shadow, freed);
+            }
+        }
+        warpPush(q.extend[cur ^ 1], &q.counts[kCountExtend0 + (cur ^ 1)], cont, path);
+        warpPush(q.shadow[cur], &q.counts[kCountShadow0 + cur], shadow, path);
+        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
+        if constexpr (MULTI) countDone(J, freed, r);
+    }
+}
+
+// render.cpp:390-413: each pixel adds the chunk's samples in index order.
+static __global__ void k_accumulate(const float4* out, Chunk C, double* acc) {
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < C.pixels;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t sBegin = C.c0 > p ? (C.c0 - p + C.pixels - 1) / C.pixels : 0;
+        const uint64_t sEnd = C.c1 > p ? (C.c1 - p + C.pixels - 1) / C.pixels : 0;
+        double r = acc[3 * p], g = acc[3 * p + 1], b = acc[3 * p + 2];
+        for (uint64_t s = sBegin; s < sEnd; ++s) {
+            const float4 o = out[s * C.pixels + p - C.c0];
+            r += o.x; g += o.y; b += o.z;
+        }
+        acc[3 * p] = r; acc[3 * p + 1] = g; acc[3 * p + 2] = b;
+    }
+}
+// Copies the chunk's radiance as packed RGB (sample-major) for stream-level comparisons.
+static __global__ void k_pack_samples(const float4* out, uint64_t n, float* dst) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const float4 o = out[i];
+        dst[3 * i] = o.x; dst[3 * i + 1] = o.y; dst[3 * i + 2] = o.z;
+    }
+}
+// render.cpp:415
+static __global__ void k_film(const double* acc, float* film, uint64_t pixels, int samples) {
+    for (uint64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * pixels; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        film[i] = static_cast<float>(acc[i] / samples);
+}
+
+// Re-runs one failing sample on one thread with full error capture (same device functions).
+static __global__ void k_trace_one(DevScene S, RenderParams P, PathSoA st, uint32_t pixel, uint32_t sample, DevError* detail,
+                            unsigned long long* scratchKey, unsigned long long* scratchRetries) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const ErrSink E{scratchKey, detail};
+    const uint32_t path = 0;
+    const uint64_t pixels = static_cast<uint64_t>(P.width) * P.height;
+    const uint64_t id = static_cast<uint64_t>(sample) * pixels + pixel;
+    const OutRef O = outOf(Chunk{id, id + 1, pixels});
+    if (!initPath(S, P, st, path, pixel, sample, false, E)) return;
+    for (int iter = 0; iter < 4 * (P.bounces + 2); ++iter) {
+        const uint32_t flags = st.flags[path];
+        const TRay r = loadRay(st, path, flags);
+        HitRec h;
+        h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
+        int err = 0;
+        const bool found = intersect<false>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0, h, err);
+        if (err) { raise(E, P, pixel, sample, err); return; }
+        st.hit_tri[path] = found ? h.tri : kNoTriangle;
+        bool cont = false, shadow = false, freed = false;
+        shadeOne<kShadeGeneric>(S, P, O, st, path, E, scratchRetries, cont, shadow, freed);
+        if (detail->code) return;
+        if (shadow) shadowOne(S, P, O, st, path, E);
+        if (detail->code || !cont) return;
+    }
+}
+
+static __global__ void k_intersect_batch(DevScene S, const cr_ray* rays, cr_hit* hits, uint8_t* found, uint64_t n, int any,
+                                  uint32_t ignore, int exact, unsigned long long* errIndex) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const cr_ray cr = rays[i];
+        TRay r;
+        r.o = v3(cr.origin); r.d = v3(cr.direction); r.tmin = cr.tmin; r.tmax = cr.tmax; r.olow = v3(cr.origin_low);
+        const cr_hit in = hits[i];
+        HitRec h{in.t, in.u, in.v, in.triangle};
+        int err = 0;
+        const bool f = any ? intersect<true>(S, r, in.t, ignore, exact != 0, h, err)
+                           : intersect<false>(S, r, in.t, ignore, exact != 0, h, err);
+        if (f) { cr_hit out = in; out.t = h.t; out.u = h.u; out.v = h.v; out.triangle = h.tri; hits[i] = out; }
+        found[i] = f ? 1 : 0;
+        if (err) atomicMin(errIndex, static_cast<unsigned long long>(i));
+    }
+}
+
+static __global__ void k_camera_rays(RenderParams P, uint32_t sample, cr_ray* out, unsigned long long* errKey) {
+    const uint64_t pixels = static_cast<uint64_t>(P.width) * P.height;
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < pixels; p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        Rng rng(sampleSeed(P.seed, p, sample));
+        const uint32_t x = static_cast<uint32_t>(p % P.width), y = static_cast<uint32_t>(p / P.width);
+        const float dx = rng.uniform(), dy = rng.uniform();
+        TRay r;
+        cr_ray o;
+        if (!cameraRay(P.camera, P.width, P.height, static_cast<float>(x) + dx, static_cast<float>(y) + dy, r)) {
+            atomicMin(errKey, static_cast<unsigned long long>(errorKey(P, static_cast<uint32_t>(p), sample)));
+            memset(&o, 0, sizeof(o));
+        } else {
+            o.origin[0] = r.o.x; o.origin[1] = r.o.y; o.origin[2] = r.o.z;
+            o.direction[0] = r.d.x; o.direction[1] = r.d.y; o.direction[2] = r.d.z;
+            o.tmin = r.tmin; o.tmax = r.tmax;
+            o.origin_low[0] = o.origin_low[1] = o.origin_low[2] = 0;
+        }
+        out[p] = o;
+    }
+}
+
+}  // namespace crg

@@ -17,7 +17,8 @@
 // order into FP64 sums (render.cpp:388-415), so the film does not depend on scheduling.
 // Precision replay (render.cpp:403-412) resets a failing path to its camera ray with split
 // origins and runs it again in the same pool.
-#include "cr_shade.cuh"
+#include "cr_kernels.cuh"
+#include "cr_driver.h"
 #include "cr_encode.h"
 #include "cr_host.h"
 
@@ -31,573 +32,43 @@
 #include <thread>
 #include <vector>
 
-// Minimum resident blocks per SM requested from the register allocator (128-thread blocks).
-// k_trace at 12 (40 registers, some spills to L1) measured ~2 % faster than at 8 or 10 on
-// the 1M-triangle workload; k_shade above 4 loses more to spills than it gains.
-#ifndef CR_TRACE_MIN_BLOCKS
-#define CR_TRACE_MIN_BLOCKS 12
-#endif
-#ifndef CR_SHADE_MIN_BLOCKS
-#define CR_SHADE_MIN_BLOCKS 4
-#endif
-
-namespace crg {
-
-// A chunk of consecutive sample ids [c0, c1); out[] holds their radiance at id - c0.
-struct Chunk {
-    uint64_t c0, c1, pixels;
-};
-
-enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatPairs = 4, kStatTris = 5,
-       kStatIssued = 6, kStatShadowPairs = 7, kStatShadowTris = 8, kStatWords = 12 };
-
-CR_D uint64_t errorKey(const RenderParams& P, uint32_t pixel, uint32_t sample) {
-    const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
-    const uint64_t tilesX = (static_cast<uint64_t>(P.width) + 15) / 16;
-    const uint64_t rank = ((y / 16) * tilesX + x / 16) * 256 + (y % 16) * 16 + (x % 16);
-    return (rank << 21) | sample;
-}
-
-// Error sink: the smallest key is kept for the report; when detail is set (single-sample
-// re-run), the full record is written there.
-struct ErrSink {
-    unsigned long long* minKey;
-    DevError* detail;
-};
-CR_D void raise(const ErrSink& E, const RenderParams& P, uint32_t pixel, uint32_t sample, int code) {
-    atomicMin(E.minKey, static_cast<unsigned long long>(errorKey(P, pixel, sample)));
-    if (E.detail) {
-        E.detail->code = code;
-        E.detail->x = static_cast<int32_t>(pixel % static_cast<uint32_t>(P.width));
-        E.detail->y = static_cast<int32_t>(pixel / static_cast<uint32_t>(P.width));
-        E.detail->sample = static_cast<int32_t>(sample);
-        E.detail->key = errorKey(P, pixel, sample);
-    }
-}
-
-// All 32 lanes call this together; lanes with pred append value to the queue.
-CR_D void warpPush(uint32_t* queue, uint32_t* counter, bool pred, uint32_t value) {
-    const unsigned mask = __ballot_sync(0xffffffffu, pred);
-    if (!mask) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (pred) queue[base + __popc(mask & ((1u << lane) - 1u))] = value;
-}
-
-CR_D float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
-
-// render.cpp:396-401 plus trace()'s initial state (render.cpp:235-239).
-CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t slot, uint32_t pixel,
-                   uint32_t sample, bool precise, const ErrSink& E) {
-    Rng rng(sampleSeed(P.seed, pixel, sample));
-    const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
-    const float dx = rng.uniform(), dy = rng.uniform();
-    TRay ray;
-    if (!cameraRay(P.camera, P.width, P.height, static_cast<float>(x) + dx, static_cast<float>(y) + dy, ray)) {
-        raise(E, P, pixel, sample, kErrUnrepresentableCameraRay);
-        return false;
-    }
-    st.ray_o[slot] = f4(ray.o, ray.tmin);
-    st.ray_d[slot] = f4(ray.d, ray.tmax);
-    st.ray_lo[slot] = make_float4(0, 0, 0, 0);
-    st.thr[slot] = make_float4(1, 1, 1, 1);          // throughput 1, etaScale 1
-    st.rad[slot] = make_float4(0, 0, 0, 0);          // radiance 0, lastPdf 0
-    st.last_pos[slot] = make_float4(0, 0, 0, 0);
-    st.absorb[slot] = make_float4(0, 0, 0, __int_as_float(-1));  // medium -1
-    st.flags[slot] = kPathLastDelta | (precise ? kPathPrecise : 0u);
-    st.rng[slot] = rng.state;
-    st.prev_tri[slot] = kNoTriangle;
-    st.pixel[slot] = pixel;
-    st.sample[slot] = sample;
-    st.depth[slot] = 0;
-    return true;
-}
-
-CR_D TRay loadRay(const PathSoA& st, uint32_t path, uint32_t flags) {
-    const float4 o = st.ray_o[path], d = st.ray_d[path];
-    TRay r;
-    r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w;
-    r.olow = (flags & kPathPrecise) ? v3(st.ray_lo[path]) : V3{};
-    return r;
-}
-
-// Ends a path: the reference's final radiance check (render.cpp:346), then the sample output.
-CR_D void finishPath(const RenderParams& P, const Chunk& C, const PathSoA& st, uint32_t path, V3 R, const ErrSink& E) {
-    const uint32_t pixel = st.pixel[path], sample = st.sample[path];
-    if (!finite3(R) || smin3(R.x, R.y, R.z) < 0) {
-        raise(E, P, pixel, sample, kErrNonFiniteRadiance);
-        R = V3{};
-    }
-    st.out[static_cast<uint64_t>(sample) * C.pixels + pixel - C.c0] = f4(R, 0);
-}
-
-// One iteration of trace()'s bounce loop (render.cpp:240-344) for one path, after its
-// closest hit is known. cont: the path continues; shadow: a shadow ray was queued (a path
-// that ends with a queued shadow ray is finished by k_trace next iteration); freed: the path
-// ended and its slot can take a new sample. CLASS specialises the code: kShadeMiss holds only
-// environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeGeneric anything.
-template <int CLASS>
-CR_D void shadeOne(const DevScene& S, const RenderParams& P, const Chunk& C, const PathSoA& st, uint32_t path,
-                   const ErrSink& E, unsigned long long* retries, bool& cont, bool& shadow, bool& freed) {
-    cont = false; shadow = false; freed = false;
-    uint32_t flags = st.flags[path];
-    const bool precise = flags & kPathPrecise;
-    const TRay ray = loadRay(st, path, flags);
-    const float4 th = st.thr[path], ra = st.rad[path], ab = st.absorb[path];
-    V3 T = v3(th), R = v3(ra), A = v3(ab);
-    float etaScale = th.w, lastPdf = ra.w;
-    int medium = __float_as_int(ab.w);
-    bool lastDelta = flags & kPathLastDelta;
-    const V3 lastPosition = v3(st.last_pos[path]);
-    const uint32_t depth = st.depth[path];
-    const uint32_t pixel = st.pixel[path], sample = st.sample[path];
-    Rng rng(st.rng[path]);
-    const uint32_t tri = st.hit_tri[path];
-    int err = 0;
-    auto finish = [&](V3 radiance) { finishPath(P, C, st, path, radiance, E); freed = true; };
-
-    if (CLASS == kShadeMiss || (CLASS == kShadeGeneric && tri == kNoTriangle)) {  // render.cpp:242-248
-        if (medium >= 0) T = T * beerLambert(A, kInf);
-        const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, environmentPdf(S, ray.d));
-        R = R + T * envRadiance(S, ray.d) * weight;
-        finish(R);
-        return;
-    }
-    // The traversal reported the triangle; t, u and v come from the same FP64 arithmetic.
-    const cr_triangle& tr = S.tris[tri];
-    const ExactSetup X = exact_setup(ray);
-    double t = 0, w1 = 0, w2 = 0, det = 1;
-    tri_exact(X, v3(tr.v[0].position), v3(tr.v[1].position), v3(tr.v[2].position), -static_cast<double>(kInf),
-              static_cast<double>(kInf), t, w1, w2, det);
-    const double hu = w1 / det, hv = w2 / det;
-    if (medium >= 0) T = T * beerLambert(A, static_cast<float>(t));
-    const Surface s = surfaceAt(S, ray.d, tri, hu, hv, err);
-    if (s.frontFace || s.doubleSided) {
-        const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, trianglePdf(S, tri, lastPosition, s.position));
-        R = R + T * s.emission * weight;
-    }
-    if (static_cast<int>(depth) == P.bounces) {
-        if (err) { raise(E, P, pixel, sample, err); }
-        finish(R);
-        return;
-    }
-    const V3 wo = -ray.d;
-    bool pending = false;
-    TRay sh;
-    V3 contrib;
-    if (CLASS == kShadeNeeNull && P.nee) {
-        skipLight(S, rng, P.env_alias != 0);  // zero BSDF: the sample cannot contribute
-    } else if (P.nee) {  // render.cpp:262-299
-        const LightSample light = sampleLight(S, s.position, rng, P.env_alias, err);
-        const bool enclosedInfinite = medium >= 0 && s.thickness <= 0 && !isfin(light.distance);
-        if (!enclosedInfinite && light.pdf > 0 && maxComponent(light.radiance) > 0) {
-            const BsdfEval bsdf = evaluateBsdf(s, wo, light.direction);
-            if (maxComponent(bsdf.value) > 0) {
-                bool ok = true;
-                if (precise) { sh.o = s.position; sh.d = light.direction; sh.tmin = 0; sh.tmax = kInf; sh.olow = s.positionLow; }
-                else ok = offsetRay(s.position, s.geometricNormal, light.direction, kInf, sh, err);
-                if (ok && isfin(light.distance)) {
-                    V3 end = light.target;
-                    if (lengthSquared(light.targetNormal) > 0) {
-                        TRay moved;
-                        ok = offsetRay(end, light.targetNormal, -light.direction, kInf, moved, err);
-                        end = moved.o;
-                    }
-                    const V3 delta = end - sh.o;
-                    sh.tmax = length(delta) * (1 - 2e-6f);
-                    sh.d = normalize(delta);
-                }
-                if (ok) {
-                    const float weight = light.delta ? 1 : powerHeuristic(light.pdf, bsdf.pdf);
-                    V3 shadowAbsorption = A;
-                    bool shadowInMedium = medium >= 0;
-                    if (s.thickness > 0 && dot(wo, s.geometricNormal) * dot(light.direction, s.geometricNormal) < 0) {
-                        shadowInMedium = s.frontFace;
-                        shadowAbsorption = s.frontFace ? absorptionCoefficient(s.attenuationColor, s.attenuationDistance) : V3{};
-                    }
-                    const V3 transmittance = shadowInMedium ? beerLambert(shadowAbsorption, light.distance) : V3{1};
-                    contrib = T * bsdf.value * light.radiance * transmittance *
-                              (fabsf(dot(s.normal, light.direction)) * weight / light.pdf);
-                    pending = true;
-                }
-            }
-        }
-    }
-    if (err) {  // an exception inside trace(): the sample fails
-        raise(E, P, pixel, sample, err);
-        finish(V3{});
-        return;
-    }
-    const uint32_t ignore = precise ? tri : kNoTriangle;
-    auto queueShadow = [&](bool dead) {
-        st.sh_o[path] = f4(sh.o, sh.tmin);
-        st.sh_d[path] = f4(sh.d, sh.tmax);
-        st.sh_lo[path] = f4(sh.olow, __uint_as_float(ignore));
-        st.sh_c[path] = f4(contrib, 0);
-        shadow = true;
-        if (dead) {
-            st.rad[path] = f4(R, lastPdf);
-            st.flags[path] = flags | kPathDead | kPathShadow;
-        }
-    };
-    const BsdfSample smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
-    if (!smp.ok()) {
-        if (pending) queueShadow(true); else finish(R);
-        return;
-    }
-    T = T * smp.weight;
-    if (!finite3(T)) {
-        raise(E, P, pixel, sample, kErrNonFiniteThroughput);
-        finish(V3{});
-        return;
-    }
-    int boundary = 0;
-    if (smp.transmitted && s.thickness > 0) {  // render.cpp:306-329
-        if (s.frontFace) {
-            if (medium >= 0) boundary = kErrNestedVolume;
-            else { medium = static_cast<int>(s.material); A = absorptionCoefficient(s.attenuationColor, s.attenuationDistance); }
-        } else {
-            if (medium < 0) boundary = kErrExitWithoutEntry;
-            else { medium = -1; A = V3{}; }
-        }
-        if (!boundary) etaScale *= smp.eta * smp.eta;
-    }
-    if (boundary) {
-        if (!precise) {  // render.cpp:404-411: replay the same sample from split origins
-            atomicAdd(retries, 1ull);
-            initPath(S, P, st, path, pixel, sample, true, E);
-            cont = true;
-            return;
-        }
-        raise(E, P, pixel, sample, boundary);
-        if (E.detail && boundary == kErrExitWithoutEntry) {
-            E.detail->depth = static_cast<int32_t>(depth);
-            E.detail->triangle = tri;
-            E.detail->material = s.material;
-            E.detail->t = t;
-            E.detail->point[0] = s.position.x; E.detail->point[1] = s.position.y; E.detail->point[2] = s.position.z;
-            E.detail->origin[0] = ray.o.x; E.detail->origin[1] = ray.o.y; E.detail->origin[2] = ray.o.z;
-            E.detail->direction[0] = ray.d.x; E.detail->direction[1] = ray.d.y; E.detail->direction[2] = ray.d.z;
-        }
-        finish(V3{});
-        return;
-    }
-    lastPdf = smp.pdf;
-    lastDelta = smp.delta;
-    TRay next;
-    if (precise) { next.o = s.position; next.d = smp.direction; next.tmin = 0; next.tmax = kInf; next.olow = s.positionLow; }
-    else if (!offsetRay(s.position, s.geometricNormal, smp.direction, kInf, next, err)) {
-        raise(E, P, pixel, sample, err);
-        finish(V3{});
-        return;
-    }
-    if (P.rr && depth >= 3) {  // render.cpp:337-343
-        const float survive = sclamp(maxComponent(T) * etaScale, 0.05f, 0.95f);
-        if (rng.uniform() >= survive) {
-            if (pending) queueShadow(true); else finish(R);
-            return;
-        }
-        T = T * (1 / survive);
-    }
-    // continue
-    st.ray_o[path] = f4(next.o, next.tmin);
-    st.ray_d[path] = f4(next.d, next.tmax);
-    if (precise) st.ray_lo[path] = f4(next.olow, 0);
-    st.thr[path] = f4(T, etaScale);
-    st.rad[path] = f4(R, lastPdf);
-    st.last_pos[path] = f4(s.position, 0);
-    st.absorb[path] = f4(A, __int_as_float(medium));
-    flags = (flags & kPathPrecise) | (lastDelta ? kPathLastDelta : 0u);
-    st.flags[path] = flags;
-    st.rng[path] = rng.state;
-    st.prev_tri[path] = ignore;
-    st.depth[path] = depth + 1;
-    if (pending) queueShadow(false);
-    cont = true;
-}
-
-// Any hit for one queued shadow ray; an unoccluded contribution is added (render.cpp:283-296).
-// Returns true when the path had ended and its slot is now free.
-template <bool COUNT = false>
-CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const Chunk& C, const PathSoA& st, uint32_t path,
-                    const ErrSink& E, unsigned long long* stats = nullptr) {
-    const float4 o = st.sh_o[path], d = st.sh_d[path], lo = st.sh_lo[path], c = st.sh_c[path];
-    TRay r;
-    r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w; r.olow = v3(lo);
-    HitRec h;
-    h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
-    int err = 0;
-    VisitCount vc;
-    const bool blocked = intersect<true, COUNT>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0,
-                                                h, err, &vc);
-    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
-    if (COUNT) {
-        atomicAdd(&stats[kStatShadowPairs], static_cast<unsigned long long>(vc.pairs));
-        atomicAdd(&stats[kStatShadowTris], static_cast<unsigned long long>(vc.tris));
-    }
-    const float4 ra = st.rad[path];
-    V3 R = v3(ra);
-    if (!blocked) R = R + v3(c);
-    const uint32_t flags = st.flags[path];
-    if (flags & kPathDead) { finishPath(P, C, st, path, R, E); return true; }
-    st.rad[path] = f4(R, ra.w);
-    return false;
-}
-
-template <bool COUNT>
-CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
-                    unsigned long long* stats) {
-    const uint32_t flags = st.flags[path];
-    const TRay r = loadRay(st, path, flags);
-    HitRec h;
-    h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
-    int err = 0;
-    VisitCount vc;
-    const bool found = intersect<false, COUNT>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
-                                               h, err, &vc);
-    st.hit_tri[path] = found ? h.tri : kNoTriangle;
-    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
-    if (COUNT) {
-        atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
-        atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
-    }
-    if (!found) return kShadeMiss;
-    return (S.nee_skip && (h.flags & kTriNeeNull)) ? kShadeNeeNull : kShadeGeneric;
-}
-
-// ---- kernels -----------------------------------------------------------------------------------
-// Every pool slot starts free (in free[1], which the first k_regen reads).
-__global__ void k_pool_init(Queues q, uint32_t pool) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pool; i += gridDim.x * blockDim.x) q.free[1][i] = i;
-    if (blockIdx.x == 0 && threadIdx.x == 0) q.counts[kCountFree1] = pool;
-}
-
-// Free slots take the next sample ids of the chunk, in order.
-__global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
-                                               unsigned long long* stats) {
-    const uint32_t n = q.counts[kCountFree0 + (cur ^ 1)];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        q.counts[kCountFree0 + cur] = 0;
-        for (int c = 0; c < kShadeClasses; ++c) q.counts[kCountShade0 + c] = 0;
-    }
-    const uint32_t* freeQ = q.free[cur ^ 1];
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-        const bool have = idx < n;
-        const uint32_t slot = have ? freeQ[idx] : 0;
-        const unsigned mask = __ballot_sync(0xffffffffu, have);
-        const int lane = threadIdx.x & 31;
-        unsigned long long first = 0;
-        if (mask) {
-            const int leader = __ffs(mask) - 1;
-            if (lane == leader) first = atomicAdd(&stats[kStatIssued], static_cast<unsigned long long>(__popc(mask)));
-            first = __shfl_sync(0xffffffffu, first, leader);
-        }
-        const uint64_t id = first + __popc(mask & ((1u << lane) - 1u));
-        bool live = false;
-        if (have && id < C.c1) {
-            const uint32_t pixel = static_cast<uint32_t>(id % C.pixels), sample = static_cast<uint32_t>(id / C.pixels);
-            live = initPath(S, P, st, slot, pixel, sample, false, E);
-            if (!live) st.out[id - C.c0] = make_float4(0, 0, 0, 0);
-        }
-        warpPush(q.extend[cur], &q.counts[kCountExtend0 + cur], live, slot);
-    }
-}
-
-// Closest hit for the live queue and any hit for last iteration's shadow rays, one launch.
-template <bool COUNT>
-__global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
-                                               unsigned long long* stats) {
-    const uint32_t nE = q.counts[kCountExtend0 + cur];
-    const uint32_t nS = q.counts[kCountShadow0 + (cur ^ 1)];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        q.counts[kCountExtend0 + (cur ^ 1)] = 0;
-        q.counts[kCountShadow0 + cur] = 0;
-        stats[kStatExtendRays] += nE;
-        stats[kStatShadowRays] += nS;
-    }
-    const uint32_t total = nE + nS;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-        bool freed = false;
-        int cls = -1;
-        uint32_t path = 0;
-        if (idx < nE) {
-            path = q.extend[cur][idx];
-            cls = closestOne<COUNT>(S, P, st, path, E, stats);
-        } else if (idx < total) {
-            path = q.shadow[cur ^ 1][idx - nE];
-            freed = shadowOne<COUNT>(S, P, C, st, path, E, stats);
-        }
-        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
-#pragma unroll
-        for (int c = 0; c < kShadeClasses; ++c) warpPush(q.shade[c], &q.counts[kCountShade0 + c], cls == c, path);
-    }
-}
-
-template <int CLASS>
-__global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
-                                               unsigned long long* stats) {
-    const uint32_t n = q.counts[kCountShade0 + CLASS];
-    const uint32_t* in = q.shade[CLASS];
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-        bool cont = false, shadow = false, freed = false;
-        uint32_t path = 0;
-        if (idx < n) {
-            path = in[idx];
-            shadeOne<CLASS>(S, P, C, st, path, E, &stats[kStatRetries], cont, shadow, freed);
-        }
-        warpPush(q.extend[cur ^ 1], &q.counts[kCountExtend0 + (cur ^ 1)], cont, path);
-        warpPush(q.shadow[cur], &q.counts[kCountShadow0 + cur], shadow, path);
-        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
-    }
-}
-
-// render.cpp:390-413: each pixel adds the chunk's samples in index order.
-__global__ void k_accumulate(const float4* out, Chunk C, double* acc) {
-    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < C.pixels;
-         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t sBegin = C.c0 > p ? (C.c0 - p + C.pixels - 1) / C.pixels : 0;
-        const uint64_t sEnd = C.c1 > p ? (C.c1 - p + C.pixels - 1) / C.pixels : 0;
-        double r = acc[3 * p], g = acc[3 * p + 1], b = acc[3 * p + 2];
-        for (uint64_t s = sBegin; s < sEnd; ++s) {
-            const float4 o = out[s * C.pixels + p - C.c0];
-            r += o.x; g += o.y; b += o.z;
-        }
-        acc[3 * p] = r; acc[3 * p + 1] = g; acc[3 * p + 2] = b;
-    }
-}
-// Copies the chunk's radiance as packed RGB (sample-major) for stream-level comparisons.
-__global__ void k_pack_samples(const float4* out, uint64_t n, float* dst) {
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const float4 o = out[i];
-        dst[3 * i] = o.x; dst[3 * i + 1] = o.y; dst[3 * i + 2] = o.z;
-    }
-}
-// render.cpp:415
-__global__ void k_film(const double* acc, float* film, uint64_t pixels, int samples) {
-    for (uint64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * pixels; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        film[i] = static_cast<float>(acc[i] / samples);
-}
-
-// Re-runs one failing sample on one thread with full error capture (same device functions).
-__global__ void k_trace_one(DevScene S, RenderParams P, PathSoA st, uint32_t pixel, uint32_t sample, DevError* detail,
-                            unsigned long long* scratchKey, unsigned long long* scratchRetries) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    const ErrSink E{scratchKey, detail};
-    const uint32_t path = 0;
-    const uint64_t pixels = static_cast<uint64_t>(P.width) * P.height;
-    const uint64_t id = static_cast<uint64_t>(sample) * pixels + pixel;
-    const Chunk C{id, id + 1, pixels};
-    if (!initPath(S, P, st, path, pixel, sample, false, E)) return;
-    for (int iter = 0; iter < 4 * (P.bounces + 2); ++iter) {
-        const uint32_t flags = st.flags[path];
-        const TRay r = loadRay(st, path, flags);
-        HitRec h;
-        h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
-        int err = 0;
-        const bool found = intersect<false>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0, h, err);
-        if (err) { raise(E, P, pixel, sample, err); return; }
-        st.hit_tri[path] = found ? h.tri : kNoTriangle;
-        bool cont = false, shadow = false, freed = false;
-        shadeOne<kShadeGeneric>(S, P, C, st, path, E, scratchRetries, cont, shadow, freed);
-        if (detail->code) return;
-        if (shadow) shadowOne(S, P, C, st, path, E);
-        if (detail->code || !cont) return;
-    }
-}
-
-__global__ void k_intersect_batch(DevScene S, const cr_ray* rays, cr_hit* hits, uint8_t* found, uint64_t n, int any,
-                                  uint32_t ignore, int exact, unsigned long long* errIndex) {
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const cr_ray cr = rays[i];
-        TRay r;
-        r.o = v3(cr.origin); r.d = v3(cr.direction); r.tmin = cr.tmin; r.tmax = cr.tmax; r.olow = v3(cr.origin_low);
-        const cr_hit in = hits[i];
-        HitRec h{in.t, in.u, in.v, in.triangle};
-        int err = 0;
-        const bool f = any ? intersect<true>(S, r, in.t, ignore, exact != 0, h, err)
-                           : intersect<false>(S, r, in.t, ignore, exact != 0, h, err);
-        if (f) { cr_hit out = in; out.t = h.t; out.u = h.u; out.v = h.v; out.triangle = h.tri; hits[i] = out; }
-        found[i] = f ? 1 : 0;
-        if (err) atomicMin(errIndex, static_cast<unsigned long long>(i));
-    }
-}
-
-__global__ void k_camera_rays(RenderParams P, uint32_t sample, cr_ray* out, unsigned long long* errKey) {
-    const uint64_t pixels = static_cast<uint64_t>(P.width) * P.height;
-    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < pixels; p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        Rng rng(sampleSeed(P.seed, p, sample));
-        const uint32_t x = static_cast<uint32_t>(p % P.width), y = static_cast<uint32_t>(p / P.width);
-        const float dx = rng.uniform(), dy = rng.uniform();
-        TRay r;
-        cr_ray o;
-        if (!cameraRay(P.camera, P.width, P.height, static_cast<float>(x) + dx, static_cast<float>(y) + dy, r)) {
-            atomicMin(errKey, static_cast<unsigned long long>(errorKey(P, static_cast<uint32_t>(p), sample)));
-            memset(&o, 0, sizeof(o));
-        } else {
-            o.origin[0] = r.o.x; o.origin[1] = r.o.y; o.origin[2] = r.o.z;
-            o.direction[0] = r.d.x; o.direction[1] = r.d.y; o.direction[2] = r.d.z;
-            o.tmin = r.tmin; o.tmax = r.tmax;
-            o.origin_low[0] = o.origin_low[1] = o.origin_low[2] = 0;
-        }
-        out[p] = o;
-    }
-}
-
-}  // namespace crg
-
 // =============================================================================================
 // Host driver
 // =============================================================================================
 using namespace crg;
+using namespace crd;
 
-namespace {
+namespace crd {
 
-struct CudaError : crh::Error {
-    CudaError(cudaError_t e, const char* what)
-        : crh::Error(e == cudaErrorMemoryAllocation ? CR_ERR_OUT_OF_MEMORY : CR_ERR_CUDA,
-                     std::string(what) + ": " + cudaGetErrorString(e)) {}
-};
-#define CR_CUDA(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) throw CudaError(e_, #call); } while (0)
-
-// Device allocation owned by a scene.
-struct DevAlloc {
-    std::vector<void*> blocks;
-    uint64_t bytes = 0;
-    template <class T> T* alloc(size_t count) {
-        if (count == 0) count = 1;
-        void* p = nullptr;
-        CR_CUDA(cudaMalloc(&p, count * sizeof(T)));
-        blocks.push_back(p);
-        bytes += count * sizeof(T);
-        return static_cast<T*>(p);
-    }
-    template <class T> T* upload(const T* src, size_t count, cudaStream_t s) {
-        T* d = alloc<T>(count);
-        if (count) CR_CUDA(cudaMemcpyAsync(d, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
-        return d;
-    }
-    void release() {
-        for (void* p : blocks) cudaFree(p);
-        blocks.clear();
-        bytes = 0;
-    }
-};
-
-int occupancyGrid(const void* kernel, int block, int device) {
-    int sms = 0, perSm = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, block, 0);
-    if (perSm < 1) perSm = 1;
-    return sms * perSm;
+cr_status fail(const std::exception& e) {
+    if (const auto* x = dynamic_cast<const crh::Error*>(&e)) return crh::set_last_error(x->status, x->what());
+    if (dynamic_cast<const std::bad_alloc*>(&e)) return crh::set_last_error(CR_ERR_OUT_OF_MEMORY, "host allocation failed");
+    return crh::set_last_error(CR_ERR_CUDA, e.what());
 }
 
-}  // namespace
+cr_gpu_tuning defaults(const cr_gpu_tuning* t) {
+    cr_gpu_tuning d{};
+    if (t) d = *t;
+    return d;
+}
+
+RenderParams makeParams(const cr_camera& camera, const cr_render_options& o, const cr_gpu_tuning& t) {
+    RenderParams P{};
+    P.width = o.width; P.height = o.height; P.samples = o.samples; P.bounces = o.bounces;
+    P.seed = o.seed; P.nee = o.next_event_estimation != 0; P.rr = o.russian_roulette != 0;
+    P.env_alias = t.env_alias; P.exact_traversal = t.exact_traversal;
+    crh::camera_setup(camera, o.width, o.height, P.camera);
+    return P;
+}
+
+int referenceWorkers(const cr_render_options& o) {  // render.cpp:361-363
+    constexpr int tileSize = 16;
+    const int tilesX = (o.width + tileSize - 1) / tileSize, tilesY = (o.height + tileSize - 1) / tileSize, tiles = tilesX * tilesY;
+    const int automatic = static_cast<int>(std::max(1u, std::thread::hardware_concurrency() / 2));
+    return std::min(tiles, o.threads ? o.threads : automatic);
+}
+
+}  // namespace crd
 
 // Render work buffers of one device: the path pool, its queues, the chunk's per-sample
 // radiance and the host staging words. Kept for the life of the process and shared by every
@@ -632,22 +103,8 @@ struct Workspace {
         work.release();
         capacity = 0;
         const size_t n = paths;
-        st.ray_o = work.alloc<float4>(n); st.ray_d = work.alloc<float4>(n); st.ray_lo = work.alloc<float4>(n);
-        st.hit_tri = work.alloc<uint32_t>(n);
-        st.thr = work.alloc<float4>(n); st.rad = work.alloc<float4>(n); st.last_pos = work.alloc<float4>(n);
-        st.absorb = work.alloc<float4>(n); st.flags = work.alloc<uint32_t>(n);
-        st.rng = work.alloc<uint64_t>(n); st.prev_tri = work.alloc<uint32_t>(n);
-        st.pixel = work.alloc<uint32_t>(n); st.sample = work.alloc<uint32_t>(n); st.depth = work.alloc<uint32_t>(n);
-        st.sh_o = work.alloc<float4>(n); st.sh_d = work.alloc<float4>(n); st.sh_lo = work.alloc<float4>(n);
-        st.sh_c = work.alloc<float4>(n);
-        for (int k = 0; k < 2; ++k) {
-            q.extend[k] = work.alloc<uint32_t>(n);
-            q.shadow[k] = work.alloc<uint32_t>(n);
-            q.free[k] = work.alloc<uint32_t>(n);
-        }
-        for (int c = 0; c < kShadeClasses; ++c) q.shade[c] = work.alloc<uint32_t>(n);
-        counts = work.alloc<uint32_t>(kCountWords);
-        q.counts = counts;
+        allocPaths(work, n, st, q);
+        counts = q.counts;
         stats = work.alloc<unsigned long long>(kStatWords);
         detail = work.alloc<DevError>(1);
         capacity = n;
@@ -680,49 +137,8 @@ Workspace& workspaceFor(int device) {
     return *ws[device];
 }
 
-struct cr_gpu_scene {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    DevAlloc geometry;  // scene data
-    DevScene dev{};
-    uint64_t triangleCount = 0;
-    crh::EnvTables env;  // host copy, for the alias table built on demand
-    DevAlloc aliasAlloc;
-    // film of the last render: FP64 sums and the float film
-    double* acc = nullptr;
-    float* film = nullptr;
-    size_t filmPixels = 0;
-    int filmWidth = 0, filmHeight = 0;  // of the last render's film (0: none yet)
-    DevAlloc filmAlloc;
-    std::mutex mutex;
-
-    ~cr_gpu_scene() {
-        if (device >= 0) cudaSetDevice(device);
-        if (stream) cudaStreamSynchronize(stream);
-        geometry.release();
-        aliasAlloc.release();
-        filmAlloc.release();
-        if (stream) cudaStreamDestroy(stream);
-    }
-
-    void ensureFilm(size_t pixels) {
-        if (pixels <= filmPixels) return;
-        CR_CUDA(cudaStreamSynchronize(stream));
-        filmAlloc.release();
-        filmPixels = 0;
-        acc = filmAlloc.alloc<double>(3 * pixels);
-        film = filmAlloc.alloc<float>(3 * pixels);
-        filmPixels = pixels;
-    }
-};
 
 namespace {
-
-cr_status fail(const std::exception& e) {
-    if (const auto* x = dynamic_cast<const crh::Error*>(&e)) return crh::set_last_error(x->status, x->what());
-    if (dynamic_cast<const std::bad_alloc*>(&e)) return crh::set_last_error(CR_ERR_OUT_OF_MEMORY, "host allocation failed");
-    return crh::set_last_error(CR_ERR_CUDA, e.what());
-}
 
 // Build the device scene: geometry in leaf order, node pairs, materials, lights, environment.
 void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_desc& env) {
@@ -942,22 +358,7 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     CR_CUDA(cudaStreamSynchronize(s));
 }
 
-RenderParams makeParams(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, const cr_gpu_tuning& t) {
-    RenderParams P{};
-    P.width = o.width; P.height = o.height; P.samples = o.samples; P.bounces = o.bounces;
-    P.seed = o.seed; P.nee = o.next_event_estimation != 0; P.rr = o.russian_roulette != 0;
-    P.env_alias = t.env_alias; P.exact_traversal = t.exact_traversal;
-    crh::camera_setup(camera, o.width, o.height, P.camera);
-    (void)g;
-    return P;
-}
 
-int referenceWorkers(const cr_render_options& o) {  // render.cpp:361-363
-    constexpr int tileSize = 16;
-    const int tilesX = (o.width + tileSize - 1) / tileSize, tilesY = (o.height + tileSize - 1) / tileSize, tiles = tilesX * tilesY;
-    const int automatic = static_cast<int>(std::max(1u, std::thread::hardware_concurrency() / 2));
-    return std::min(tiles, o.threads ? o.threads : automatic);
-}
 
 // Progressive output: after every `every` samples per pixel, the film so far, encoded.
 struct Frames {
@@ -978,7 +379,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     const uint64_t total = pixels * static_cast<uint64_t>(o.samples);
     RenderParams P;
     try {
-        P = makeParams(g, camera, o, tuning);
+        P = makeParams(camera, o, tuning);
     } catch (const crh::Error& e) {
         // The reference throws these from Camera::generate inside the first sample.
         throw crh::Error(CR_ERR_RENDER, std::string("Pixel (0,0), sample 0: ") + e.what());
@@ -1028,7 +429,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         W.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
         W.gridShadeLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
         W.gridShadeMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
-        W.gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen), 128, g.device);
+        W.gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen<false>), 128, g.device);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
         W.gridSmall = sms * 8;
@@ -1077,14 +478,14 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     if (timePhases) { CR_CUDA(cudaEventRecord(W.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
                     ++launches;
                 };
-                rec(2, [&] { k_regen<<<W.gridRegen, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
+                rec(2, [&] { k_regen<false><<<W.gridRegen, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
                 rec(0, [&] {
-                    if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats);
-                    else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats);
+                    if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{});
+                    else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{});
                 });
-                rec(1, [&] { k_shade<kShadeMiss><<<W.gridShadeMiss, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
-                rec(1, [&] { k_shade<kShadeNeeNull><<<W.gridShadeLight, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
-                rec(1, [&] { k_shade<kShadeGeneric><<<W.gridShade, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats); });
+                rec(1, [&] { k_shade<kShadeMiss><<<W.gridShadeMiss, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}); });
+                rec(1, [&] { k_shade<kShadeNeeNull><<<W.gridShadeLight, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}); });
+                rec(1, [&] { k_shade<kShadeGeneric><<<W.gridShade, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}); });
                 cur ^= 1;
                 ++iter;
                 ++iterations;
@@ -1266,7 +667,7 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
     const cr_gpu_tuning tuning{};
     RenderParams P;
     try {
-        P = makeParams(g, camera, o, tuning);
+        P = makeParams(camera, o, tuning);
     } catch (const crh::Error& e) {
         throw crh::Error(CR_ERR_RENDER, std::string("Pixel (0,0), sample 0: ") + e.what());
     }
@@ -1281,7 +682,7 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
     const int gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
     const int gridLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
     const int gridMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
-    const int gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen), 128, g.device);
+    const int gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen<false>), 128, g.device);
     const int gridSmall = sms * 8;
     // The workspace keeps the previous call's contents: clear what must start at zero.
     CR_CUDA(cudaMemsetAsync(L.acc, 0, 3 * pixels * sizeof(double), s));
@@ -1308,11 +709,11 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
         int cur = 0;
         for (;;) {
             for (int b = 0; b < 8; ++b) {
-                k_regen<<<gridRegen, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
-                k_trace<false><<<gridTrace, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
-                k_shade<kShadeMiss><<<gridMiss, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
-                k_shade<kShadeNeeNull><<<gridLight, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
-                k_shade<kShadeGeneric><<<gridShade, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats);
+                k_regen<false><<<gridRegen, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{}, 1);
+                k_trace<false><<<gridTrace, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                k_shade<kShadeMiss><<<gridMiss, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                k_shade<kShadeNeeNull><<<gridLight, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                k_shade<kShadeGeneric><<<gridShade, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
                 launches += 5;
                 cur ^= 1;
                 ++iter;
@@ -1367,11 +768,6 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
     }
 }
 
-cr_gpu_tuning defaults(const cr_gpu_tuning* t) {
-    cr_gpu_tuning d{};
-    if (t) d = *t;
-    return d;
-}
 
 }  // namespace
 
@@ -1450,7 +846,7 @@ cr_status cr_gpu_camera_rays(cr_gpu_scene* g, const cr_camera* camera, const cr_
         std::lock_guard<std::mutex> lock(g->mutex);
         crh::validate_options(*options);
         const cr_gpu_tuning t{};
-        RenderParams P = makeParams(*g, *camera, *options, t);
+        RenderParams P = makeParams(*camera, *options, t);
         CR_CUDA(cudaSetDevice(g->device));
         cudaStream_t s = g->stream;
         const uint64_t pixels = static_cast<uint64_t>(options->width) * options->height;

@@ -368,6 +368,75 @@ cr_status cr_gpu_render_progressive(cr_gpu_scene* scene, const cr_camera* camera
                                     float* film_rgb, cr_render_stats* stats,
                                     const cr_gpu_tuning* tuning);
 
+/* ---- many renders in one path pool ------------------------------------------------------------
+ * No counterpart in the reference, which renders one image per cr::render call. The engine
+ * runs the paths of many jobs (scene, camera, options) in one shared pool on one device: free
+ * path slots take the next samples of whichever jobs have samples left, so small and large
+ * jobs keep the GPU full together. Each job's samples run on its own streams and its pixel
+ * sums are added in sample order, so every job's film is exactly the film cr_gpu_render
+ * returns for it alone, whatever else shares the pool. */
+typedef struct cr_job {
+    /* inputs */
+    cr_gpu_scene* scene;          /* every job of one batch or server on the same device     */
+    cr_camera camera;
+    cr_render_options options;
+    float* film_rgb;              /* host, width*height*3 floats, or NULL                     */
+    uint32_t every_samples;       /* > 0: on_frame after every N samples per pixel            */
+    int32_t format;               /* cr_encode_format of the frames                           */
+    float exposure;               /* of CR_ENCODE_SRGB8 frames                                */
+    cr_frame_fn on_frame;         /* called on the engine's thread; may be NULL               */
+    void* user;
+    /* results, written when the job ends */
+    cr_status status;
+    cr_render_stats stats;        /* camera_samples, boundary_retries, workers, chunks, seconds */
+    double submitted_at;          /* seconds on the engine's clock                            */
+    double started_at;            /* admitted: buffers allocated, samples may start           */
+    double first_frame_at;        /* first progressive frame (0 without frames)               */
+    double finished_at;
+    char error[256];              /* the failure text, as cr_gpu_last_error would give it     */
+} cr_job;
+
+typedef struct cr_engine_tuning {
+    uint32_t pool_paths;          /* path slots; 0: 2^24                                      */
+    uint32_t range_samples;       /* most samples per issue range; 0: 2^22                    */
+    uint32_t refill_interval;     /* iterations between refills of freed slots; 0: 1          */
+    uint32_t iterations_per_step; /* iterations between host checks (even); 0: 8              */
+    int32_t use_graphs;           /* 1: launch each step as one captured CUDA graph           */
+    int32_t reserved;
+    uint64_t memory_budget;       /* bytes of job buffers admitted at once; 0: 150 GB          */
+} cr_engine_tuning;
+
+typedef struct cr_engine_stats {
+    double seconds;               /* wall time the engine was working                         */
+    uint64_t camera_samples;      /* of finished jobs                                         */
+    uint64_t iterations, launches, extend_rays, shadow_rays;
+    uint32_t jobs_done, jobs_failed, peak_jobs, graph_steps;
+} cr_engine_stats;
+
+/* Renders every job in one shared pool and returns when all have ended. The call's status is
+ * CR_OK when every job succeeded; each job's own status and error say how it ended. */
+cr_status cr_gpu_render_batch(cr_job* jobs, uint32_t count, const cr_engine_tuning* tuning,
+                              cr_engine_stats* stats);
+
+/* Picks pool size, refill interval and iterations per step for a batch by timing short trial
+ * renders (the jobs at 1 sample per pixel) of candidate settings. The jobs are not modified. */
+cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tuning* tuning);
+
+/* Continuous batching: a server owns an engine thread on `device`. Jobs submitted while
+ * others run join the pool as soon as the memory budget admits them; their samples share the
+ * pool with the jobs already running. A submitted cr_job must stay valid until it has ended
+ * (cr_server_wait returned for it, or the server was destroyed). */
+typedef struct cr_server cr_server;
+cr_status cr_server_create(int device, const cr_engine_tuning* tuning, cr_server** out);
+cr_status cr_server_submit(cr_server* server, cr_job* job, uint64_t* ticket);
+/* Waits until the job has ended (returns its status) or timeout_seconds pass
+ * (CR_ERR_DEVICE_TIMEOUT, the job keeps running). timeout < 0 waits without limit. */
+cr_status cr_server_wait(cr_server* server, uint64_t ticket, double timeout_seconds);
+cr_status cr_server_stats(cr_server* server, cr_engine_stats* stats);
+double cr_server_clock(cr_server* server);  /* seconds on the engine's clock */
+/* Finishes the submitted jobs, stops the thread and frees the engine. */
+cr_status cr_server_destroy(cr_server* server);
+
 #ifdef __cplusplus
 }
 #endif

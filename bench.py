@@ -40,6 +40,15 @@ def parse():
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-spp", type=int, default=4)
+    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "serve"],
+                    help="grid: the 1M-triangle 1080p render (default); batch: 64 uneven scenes in one pool "
+                         "against one by one; serve: a Poisson request stream through the server")
+    ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream (2000 for the full run)")
+    ap.add_argument("--rate", type=float, default=40.0, help="serve: arrivals per second")
+    ap.add_argument("--literal-clutter", action="store_true",
+                    help="batch/serve: keep config 1's triangle sizes at every triangle count")
+    ap.add_argument("--mix-scale", type=float, default=1.0,
+                    help="batch/serve: scale every job's width and height (quick runs)")
     return ap.parse_args()
 
 
@@ -321,10 +330,145 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def mix_scenes(env_size=None, literal=False):
+    """The 64 uneven scenes of the multi-scene mix on the device: [(GpuScene, camera)]."""
+    import crgpu
+    import workloads
+    out = []
+    for i, (count, seed, _, _) in enumerate(workloads.uneven_scene_mix()):
+        sc = workloads.cluttered_room_scene(count, seed, literal=literal)
+        tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
+        env = None
+        if env_size:
+            env = crgpu.env_desc(image=workloads.sky_image(width=env_size[0], height=env_size[1], seed=seed + 5))
+        out.append((crgpu.GpuScene(tris, sc["materials"], env=env), sc["camera"]))
+    return out
+
+
+def run_batch(args):
+    """64 scenes of 10^3-2x10^6 triangles, each job at its own resolution and sample count,
+    rendered in one shared pool (autotuned) against one cr_gpu_render after another."""
+    import crgpu
+    import workloads
+    mix = [(c, s, (max(1, int(w * args.mix_scale)), max(1, int(h * args.mix_scale))), spp)
+           for c, s, (w, h), spp in workloads.uneven_scene_mix()]
+    t0 = time.perf_counter()
+    scenes = mix_scenes(literal=args.literal_clutter)
+    prep = time.perf_counter() - t0
+
+    def jobs():
+        return [crgpu.JobSpec(scenes[i][0], scenes[i][1],
+                              crgpu.Options.make(width=w, height=h, samples=spp, bounces=12, seed=42), want_film=False)
+                for i, (_, _, (w, h), spp) in enumerate(mix)]
+
+    samples = sum(w * h * spp for _, _, (w, h), spp in mix)
+    t0 = time.perf_counter()
+    tuning = crgpu.autotune_batch(jobs())
+    tune_s = time.perf_counter() - t0
+    for _ in range(max(0, args.warmup)):
+        crgpu.render_batch(jobs(), tuning)
+    secs, est = [], None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        est = crgpu.render_batch(jobs(), tuning)
+        secs.append(time.perf_counter() - t0)
+    value = samples * len(secs) / sum(secs) / 1e6
+    # one by one: each job through cr_gpu_render_resident, in the same order
+    t0 = time.perf_counter()
+    for i, (_, _, (w, h), spp) in enumerate(mix):
+        scenes[i][0].render_resident(scenes[i][1], crgpu.Options.make(width=w, height=h, samples=spp, bounces=12, seed=42))
+    single_s = time.perf_counter() - t0
+    one_by_one = samples / single_s / 1e6
+    line = {
+        "metric": "aggregate Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded procedural scenes)",
+        "config": {"workload": "batch-64-uneven-scenes", "scenes": len(mix), "triangles": int(sum(m[0] for m in mix)),
+                   "samples": int(samples), "bounces": 12, "timing": "wall clock around cr_gpu_render_batch",
+                   "clutter": "literal config-1 sizes" if args.literal_clutter else "area-preserving sizes",
+                   "mix_scale": args.mix_scale},
+        "one_by_one": {"value": one_by_one, "unit": "Msamples/s", "seconds": single_s},
+        "speedup_vs_one_by_one": value / one_by_one,
+        "tuning": tuning.as_dict(), "autotune_seconds": tune_s, "scene_prep_seconds": prep,
+        "engine": est,
+    }
+    print(json.dumps(line))
+    for g, _ in scenes:
+        g.close()
+
+
+def run_serve(args):
+    """A Poisson request stream over the 64-scene mix (1024x512 sky per scene) through the
+    server: time to the first 4-spp frame and to completion, throughput against the same
+    requests rendered as one batch."""
+    import crgpu
+    import workloads
+    stream = [(t, si, (max(1, int(w * args.mix_scale)), max(1, int(h * args.mix_scale))), spp)
+              for t, si, (w, h), spp in workloads.request_stream(count=args.requests, rate=args.rate)]
+    scenes = mix_scenes(env_size=(1024, 512), literal=args.literal_clutter)
+
+    def spec(r):
+        _, si, (w, h), spp = r
+        return crgpu.JobSpec(scenes[si][0], scenes[si][1], crgpu.Options.make(width=w, height=h, samples=spp, bounces=12,
+                                                                                 seed=42), every=4, fmt=crgpu.ENCODE_SRGB8,
+                             want_film=False, keep_frames=False)
+
+    samples = sum(w * h * spp for _, _, (w, h), spp in stream)
+    # warm-up: a few requests through a server, then the measured stream
+    srv = crgpu.Server(0)
+    warm = [spec(r) for r in stream[: max(1, args.warmup)]]
+    for t in [srv.submit(j) for j in warm]:
+        srv.wait(t)
+    specs = [spec(r) for r in stream]
+    tickets = []
+    base = time.perf_counter()
+    for r, sp in zip(stream, specs):
+        delay = base + r[0] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        tickets.append(srv.submit(sp))
+    for t in tickets:
+        srv.wait(t)
+    sstats = srv.stats()
+    srv.close()
+    sub = np.array([sp.times["submitted"] for sp in specs])
+    first = np.array([sp.times["first_frame"] for sp in specs])
+    fin = np.array([sp.times["finished"] for sp in specs])
+    ok = np.array([sp.status == 0 for sp in specs])
+    ttff, ttc = (first - sub)[ok], (fin - sub)[ok]
+    served = samples / (fin.max() - sub.min()) / 1e6
+    # the same requests as one batch
+    t0 = time.perf_counter()
+    crgpu.render_batch([spec(r) for r in stream])
+    batched = samples / (time.perf_counter() - t0) / 1e6
+    pct = lambda a, q: float(np.percentile(a, q)) * 1e3
+    line = {
+        "metric": "request latency p50/p99 ms", "value": pct(ttc, 99), "unit": "ms (p99 time-to-completion)",
+        "n_gpus": 1, "steps": 1, "warmup": len(warm), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic (seeded procedural scenes, Poisson arrivals)",
+        "config": {"workload": "serve-poisson", "requests": len(stream), "rate_per_s": args.rate, "scenes": len(scenes),
+                   "env": "1024x512 per scene", "frames": "sRGB8 every 4 spp", "samples": int(samples),
+                   "clutter": "literal config-1 sizes" if args.literal_clutter else "area-preserving sizes",
+                   "mix_scale": args.mix_scale},
+        "time_to_first_4spp_ms": {"p50": pct(ttff, 50), "p99": pct(ttff, 99)},
+        "time_to_completion_ms": {"p50": pct(ttc, 50), "p99": pct(ttc, 99)},
+        "throughput": {"served": served, "batched": batched, "unit": "Msamples/s", "served_over_batched": served / batched},
+        "offered_load_msamples_per_s": samples / max(1e-9, stream[-1][0]) / 1e6,
+        "failed": int((~ok).sum()), "server": sstats,
+    }
+    print(json.dumps(line))
+    for g, _ in scenes:
+        g.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

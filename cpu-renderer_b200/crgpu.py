@@ -158,12 +158,14 @@ class Job(C.Structure):
 
 class EngineTuning(C.Structure):
     _fields_ = [("pool_paths", C.c_uint32), ("range_samples", C.c_uint32), ("refill_interval", C.c_uint32),
-                ("iterations_per_step", C.c_uint32), ("use_graphs", C.c_int32), ("reserved", C.c_int32),
-                ("memory_budget", C.c_uint64)]
+                ("iterations_per_step", C.c_uint32), ("use_graphs", C.c_int32), ("issue_policy", C.c_int32),
+                ("memory_budget", C.c_uint64), ("refill_free_percent", C.c_uint32), ("reserved", C.c_uint32)]
 
     @classmethod
-    def make(cls, pool_paths=0, range_samples=0, refill_interval=0, iterations_per_step=0, use_graphs=1, memory_budget=0):
-        return cls(pool_paths, range_samples, refill_interval, iterations_per_step, use_graphs, 0, memory_budget)
+    def make(cls, pool_paths=0, range_samples=0, refill_interval=0, iterations_per_step=0, use_graphs=1, memory_budget=0,
+             issue_policy=0, refill_free_percent=0):
+        return cls(pool_paths, range_samples, refill_interval, iterations_per_step, use_graphs, issue_policy, memory_budget,
+                   refill_free_percent, 0)
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -338,6 +340,7 @@ class GpuScene:
         e = env if env is not None else env_desc()
         h = C.c_void_p()
         check(lib.cr_gpu_scene_create(C.byref(d), C.byref(e), device, C.byref(h)))
+        self._arrays = None  # the library keeps device copies, never the caller's pointers
         self.handle = h
         self.triangle_count = len(t)
 

@@ -7,9 +7,9 @@
 //   admit     a job gets a slot in the device job tables (its scene's DevScene and its
 //             RenderParams), FP64 pixel sums and a film, if the memory budget allows
 //   issue     the jobs' remaining samples are cut into ranges (at most range_samples, never
-//             across a progressive frame boundary) and appended to the issue list, round
-//             robin over the jobs, while the per-sample radiance arena has room and the pool
-//             is not already fed a pool's worth ahead
+//             across a progressive frame boundary) and appended to the issue list, each to
+//             the job with the fewest samples per pixel issued, while the per-sample
+//             radiance arena has room and the pool is not already fed a pool's worth ahead
 //   run       iterations_per_step iterations of k_regen / k_trace / k_shade x3 (one CUDA
 //             graph when use_graphs), k_regen refilling freed slots every refill_interval
 //   complete  finished-sample counters are read back; a job's ranges are summed into its
@@ -51,19 +51,24 @@ struct EngineConfig {
     uint64_t rangeSamples = uint64_t{1} << 22;
     uint64_t outSamples = 0;
     uint32_t refill = 1;
+    uint32_t refillPercent = 0;
     uint32_t iters = 8;
     bool graphs = true;
+    int policy = 0;  // 1: jobs in order, 2: fewest samples per pixel first
     uint64_t budget = 150ull << 30;
 };
 
-EngineConfig makeConfig(const cr_engine_tuning* t) {
+EngineConfig makeConfig(const cr_engine_tuning* t, int defaultPolicy) {
     EngineConfig c;
+    c.policy = defaultPolicy;
     if (t) {
         if (t->pool_paths) c.pool = t->pool_paths;
         if (t->range_samples) c.rangeSamples = t->range_samples;
         if (t->refill_interval) c.refill = t->refill_interval;
+        c.refillPercent = std::min<uint32_t>(100, t->refill_free_percent);
         if (t->iterations_per_step) c.iters = t->iterations_per_step;
         c.graphs = t->use_graphs != 0;
+        if (t->issue_policy == 1 || t->issue_policy == 2) c.policy = t->issue_policy;
         if (t->memory_budget) c.budget = t->memory_budget;
     }
     c.pool = std::max<uint64_t>(1024, (c.pool + 127) / 128 * 128);
@@ -120,7 +125,8 @@ struct Active {
 
 class Engine {
   public:
-    Engine(int device, const cr_engine_tuning* tuning) : device_(device), cfg_(makeConfig(tuning)), arena_(0) {
+    Engine(int device, const cr_engine_tuning* tuning, int defaultPolicy)
+        : device_(device), cfg_(makeConfig(tuning, defaultPolicy)), arena_(0) {
         CR_CUDA(cudaSetDevice(device_));
         CR_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
         start_ = std::chrono::steady_clock::now();
@@ -129,10 +135,10 @@ class Engine {
         st_.out = pool_.alloc<float4>(cfg_.outSamples);
         rangeOf_ = pool_.alloc<uint32_t>(cfg_.pool);
         stats_ = pool_.alloc<unsigned long long>(kStatWords);
-        scenes_ = pool_.alloc<DevScene>(kMaxJobSlots);
-        params_ = pool_.alloc<RenderParams>(kMaxJobSlots);
         errKeys_ = pool_.alloc<unsigned long long>(kMaxJobSlots);
         retries_ = pool_.alloc<unsigned long long>(kMaxJobSlots);
+        scenes_ = pool_.alloc<DevScene>(kMaxJobSlots);
+        params_ = pool_.alloc<RenderParams>(kMaxJobSlots);
         ranges_ = pool_.alloc<IssueRange>(kMaxRanges);
         done_ = pool_.alloc<unsigned long long>(kMaxRanges);
         ctl_ = pool_.alloc<unsigned long long>(4);  // [0] issue end, [1] range count, [2..3] issued
@@ -166,6 +172,7 @@ class Engine {
         hParams_.resize(kMaxJobSlots);
         J_.scenes = scenes_; J_.params = params_; J_.ranges = ranges_; J_.ctl = ctl_; J_.issued = ctl_ + 2;
         J_.done = done_; J_.errKeys = errKeys_; J_.retries = retries_; J_.range = rangeOf_;
+        J_.refillMin = static_cast<uint32_t>(cfg_.pool * cfg_.refillPercent / 100);
     }
 
     ~Engine() {
@@ -355,33 +362,41 @@ class Engine {
             firstOpen_ = 0;
             closed_.clear();
         }
-        bool progress = true;
-        while (progress && issueEnd_ - issuedPos_ < cfg_.pool && rangeCount_ < kMaxRanges) {
-            progress = false;
-            for (auto& a : active_) {  // one range per job per pass: round robin
+        // Next range: policy 1 feeds the earliest admitted job to its end before the next, so the
+        // pool's paths stay on few scenes (their BVHs stay in cache); policy 2 feeds the job with
+        // the fewest samples per pixel issued (ties: the earliest admitted), so a job that just
+        // arrived gets its first frame's samples ahead of the later frames of running jobs.
+        while (issueEnd_ - issuedPos_ < cfg_.pool && rangeCount_ < kMaxRanges) {
+            Active* best = nullptr;
+            for (auto& a : active_) {
                 if (a.failed || a.issued >= a.total) continue;
-                if (issueEnd_ - issuedPos_ >= cfg_.pool || rangeCount_ >= kMaxRanges) break;
-                uint64_t n = std::min<uint64_t>(cfg_.rangeSamples, a.total - a.issued);
-                if (a.frameSamples) n = std::min<uint64_t>(n, (a.issued / a.frameSamples + 1) * a.frameSamples - a.issued);
-                uint64_t at = 0;
-                if (!arena_.take(n, at)) return;
-                IssueRange& R = hRanges_[rangeCount_];
-                R.start = issueEnd_;
-                R.c0 = a.issued;
-                R.c1 = a.issued + n;
-                R.outBase = at;
-                R.pixels = a.pixels;
-                R.job = a.slot;
-                R.pad = 0;
-                a.ranges.push_back(rangeCount_);
-                closed_.push_back(false);
-                ++a.chunks;
-                ++rangeCount_;
-                ++openRanges_;
-                issueEnd_ += n;
-                a.issued += n;
-                progress = true;
+                if (cfg_.policy == 1) { best = &a; break; }  // the earliest admitted job with samples left
+                // a.issued / a.pixels < best->issued / best->pixels, without division
+                if (!best || static_cast<long double>(a.issued) * best->pixels <
+                                 static_cast<long double>(best->issued) * a.pixels)
+                    best = &a;
             }
+            if (!best) return;
+            Active& a = *best;
+            uint64_t n = std::min<uint64_t>(cfg_.rangeSamples, a.total - a.issued);
+            if (a.frameSamples) n = std::min<uint64_t>(n, (a.issued / a.frameSamples + 1) * a.frameSamples - a.issued);
+            uint64_t at = 0;
+            if (!arena_.take(n, at)) return;
+            IssueRange& R = hRanges_[rangeCount_];
+            R.start = issueEnd_;
+            R.c0 = a.issued;
+            R.c1 = a.issued + n;
+            R.outBase = at;
+            R.pixels = a.pixels;
+            R.job = a.slot;
+            R.pad = 0;
+            a.ranges.push_back(rangeCount_);
+            closed_.push_back(false);
+            ++a.chunks;
+            ++rangeCount_;
+            ++openRanges_;
+            issueEnd_ += n;
+            a.issued += n;
         }
     }
 
@@ -624,7 +639,7 @@ cr_status runBatch(cr_job* jobs, uint32_t count, const cr_engine_tuning* tuning,
     for (uint32_t i = 0; i < count; ++i)
         if (jobs[i].scene) { device = jobs[i].scene->device; break; }
     if (device < 0) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "no job has a scene");
-    Engine e(device, tuning);
+    Engine e(device, tuning, 1);
     for (uint32_t i = 0; i < count; ++i) e.submit(&jobs[i]);
     try {
         while (!e.idle()) e.step();
@@ -658,25 +673,23 @@ cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tu
             j.every_samples = 0;
             j.on_frame = nullptr;
         }
-        const uint32_t pools[] = {1u << 22, 1u << 23, 1u << 24};
-        const uint32_t refills[] = {1, 2, 4};
-        const uint32_t steps[] = {8, 16};
+        const uint32_t pools[] = {1u << 22, 1u << 24};
+        const uint32_t percents[] = {0, 50, 90};
         cr_engine_tuning best = *tuning;
         double bestSeconds = 1e300;
         for (uint32_t pool : pools)
-            for (uint32_t refill : refills)
-                for (uint32_t iters : steps) {
-                    if (iters % refill) continue;
-                    cr_engine_tuning t = *tuning;
-                    t.pool_paths = pool;
-                    t.refill_interval = refill;
-                    t.iterations_per_step = iters;
-                    const auto t0 = std::chrono::steady_clock::now();
-                    const cr_status st = runBatch(trial.data(), count, &t, nullptr);
-                    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-                    if (st != CR_OK) return st;
-                    if (sec < bestSeconds) { bestSeconds = sec; best = t; }
-                }
+            for (uint32_t pct : percents) {
+                cr_engine_tuning t = *tuning;
+                t.pool_paths = pool;
+                t.refill_interval = 1;
+                t.refill_free_percent = pct;
+                t.iterations_per_step = 8;
+                const auto t0 = std::chrono::steady_clock::now();
+                const cr_status st = runBatch(trial.data(), count, &t, nullptr);
+                const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                if (st != CR_OK) return st;
+                if (sec < bestSeconds) { bestSeconds = sec; best = t; }
+            }
         *tuning = best;
         return CR_OK;
     } catch (const std::exception& e) { return fail(e); }
@@ -686,7 +699,7 @@ cr_status cr_server_create(int device, const cr_engine_tuning* tuning, cr_server
     try {
         if (!out) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
         auto srv = std::make_unique<cr_server>();
-        srv->engine = std::make_unique<Engine>(device, tuning);
+        srv->engine = std::make_unique<Engine>(device, tuning, 2);
         cr_server* s = srv.get();
         s->thread = std::thread([s] {
             try {

@@ -51,6 +51,7 @@ struct JobTable {
     unsigned long long* errKeys;     // [job slot] smallest error key
     unsigned long long* retries;     // [job slot] precision replays
     uint32_t* range;                 // [path slot] the path's range
+    uint32_t refillMin;              // refill only when at least this many slots are free
 };
 
 enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatPairs = 4, kStatTris = 5,
@@ -459,7 +460,7 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
         const unsigned long long end = J.ctl[0];
         const uint32_t rangeCount = static_cast<uint32_t>(J.ctl[1]);
         const uint64_t avail = end > first ? end - first : 0;
-        const uint32_t claimed = refill ? static_cast<uint32_t>(avail < n ? avail : n) : 0u;
+        const uint32_t claimed = refill && n >= J.refillMin ? static_cast<uint32_t>(avail < n ? avail : n) : 0u;
         if (blockIdx.x == 0 && threadIdx.x == 0) J.issued[cur] = first + claimed;
         for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
             const uint32_t idx = base + threadIdx.x;

@@ -13,6 +13,14 @@ sphere_grid_scene   1920x1080, 64 spp, 16 bounces: 20x20 closed, radially displa
                     smooth closed dielectrics (IOR U[1.3,1.7]). A 2048x1024 RGB equirect sky of
                     log-normal (mu=0, sigma=1) texels plus a 0.5-degree sun disk of radiance 5e4.
 
+cluttered_room_scene / uneven_scene_mix
+                    the multi-scene mixes: config-1 rooms whose random triangles number from
+                    10^3 to 2x10^6 (log-uniform over the mix; sizes shrink by sqrt(64/n) so the
+                    clutter's area stays the room's, unless literal), drawn from a palette of 64
+                    materials with the room's 70/30 conductor/dielectric split; each job draws
+                    a resolution from {256^2, 512^2, 1024^2, 1920x1080}, samples from
+                    {1, 4, 16, 64}, 12 bounces.
+
 All draws come from numpy's PCG64 with fixed seeds, so every call returns identical arrays.
 Triangles are returned un-finalized (Scene::finalize computes areas and normals).
 """
@@ -235,3 +243,66 @@ def sphere_grid_scene(seed=GRID_SEED, width=1920, height=1080, samples=64, bounc
     return dict(triangles=triangles, materials=mats, lights=None, camera=camera, options=options,
                 env_image=sky_image() if sky else None,
                 name="sphere-grid-1M-1920x1080-64spp-d16")
+
+
+MIX_SEED = 0x5EED0003
+MIX_RESOLUTIONS = ((256, 256), (512, 512), (1024, 1024), (1920, 1080))
+MIX_SAMPLES = (1, 4, 16, 64)
+
+
+def cluttered_room_scene(triangle_count, seed, literal=False):
+    """A config-1 room (walls, two emitters) holding triangle_count - 24 random triangles
+    (vertices in the interior) over a 64-material palette. The room's own random triangles
+    have edges 0.05-0.4 and area >= 1e-4 for 64 of them; with `literal` every scene keeps
+    those sizes, otherwise they shrink by sqrt(64 / n) so that n triangles cover the room's
+    area of clutter (at 2x10^6 literal triangles thousands of triangles overlap every point
+    of the room and every ray tests thousands of them)."""
+    base = room_scene(seed)
+    rng = np.random.default_rng(seed + 1)
+    walls = base["triangles"][:24]
+    n = max(0, int(triangle_count) - len(walls))
+    k = 1.0 if literal or n <= 64 else math.sqrt(64.0 / n)
+    ilo = np.array([-0.9, 0.1, -0.9]); ihi = np.array([0.9, 1.9, 0.9])
+    chunks, have = [], 0
+    while have < n:
+        m = int((n - have) * 1.6) + 64
+        v0 = rng.uniform(ilo, ihi, size=(m, 3))
+        d = rng.normal(size=(m, 2, 3))
+        d /= np.linalg.norm(d, axis=2, keepdims=True)
+        lens = rng.uniform(0.05 * k, 0.4 * k, size=(m, 2, 1))
+        v1 = v0 + lens[:, 0] * d[:, 0]
+        v2 = v0 + lens[:, 1] * d[:, 1]
+        e = np.linalg.norm(v2 - v1, axis=1)
+        area = 0.5 * np.linalg.norm(np.cross(v1 - v0, v2 - v0), axis=1)
+        inside = np.all((v1 > ilo) & (v1 < ihi) & (v2 > ilo) & (v2 < ihi), axis=1)
+        ok = (e >= 0.05 * k) & (e <= 0.4 * k) & (area >= 1e-4 * k * k) & inside
+        pts = np.stack([v0, v1, v2], axis=1)[ok][: n - have]
+        chunks.append(pts)
+        have += len(pts)
+    pts = np.concatenate(chunks) if chunks else np.zeros((0, 3, 3))
+    tris = new_triangles(len(walls) + n)
+    tris[: len(walls)] = walls
+    tris["v"]["position"][len(walls):] = pts.astype(np.float32)
+    palette = base["materials"][4:]  # the room's 64 random materials: 70% conductors, 30% dielectrics
+    tris["material"][len(walls):] = 4 + rng.integers(0, len(palette), size=n)
+    return dict(triangles=tris, materials=base["materials"], camera=base["camera"], name=f"room-{len(tris)}tri")
+
+
+def uneven_scene_mix(count=64, lo=1e3, hi=2e6, seed=MIX_SEED):
+    """Triangle counts (log-uniform in [lo, hi]) and per-job draws for `count` scenes:
+    returns [(triangle_count, scene_seed, (width, height), samples)]."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), size=count)).astype(np.int64)
+    res = rng.integers(0, len(MIX_RESOLUTIONS), size=count)
+    spp = rng.integers(0, len(MIX_SAMPLES), size=count)
+    return [(int(counts[i]), int(seed + 17 * (i + 1)), MIX_RESOLUTIONS[res[i]], MIX_SAMPLES[spp[i]]) for i in range(count)]
+
+
+def request_stream(count=2000, rate=40.0, scenes=64, seed=MIX_SEED + 1):
+    """A Poisson request stream over the mix: [(arrival seconds, scene index, (w, h), samples)]."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    sc = rng.integers(0, scenes, size=count)
+    res = rng.integers(0, len(MIX_RESOLUTIONS), size=count)
+    spp = rng.integers(0, len(MIX_SAMPLES), size=count)
+    return [(float(t[i]), int(sc[i]), MIX_RESOLUTIONS[res[i]], MIX_SAMPLES[spp[i]]) for i in range(count)]

@@ -402,8 +402,15 @@ typedef struct cr_engine_tuning {
     uint32_t refill_interval;     /* iterations between refills of freed slots; 0: 1          */
     uint32_t iterations_per_step; /* iterations between host checks (even); 0: 8              */
     int32_t use_graphs;           /* 1: launch each step as one captured CUDA graph           */
-    int32_t reserved;
+    int32_t issue_policy;         /* 0: automatic (batch: 1, server: 2); 1: jobs in order, each
+                                     fed to the end before the next starts (the pool's paths
+                                     stay on few scenes: throughput); 2: the job with the fewest
+                                     samples per pixel issued first (a new job's first frame
+                                     goes ahead: latency)                                      */
     uint64_t memory_budget;       /* bytes of job buffers admitted at once; 0: 150 GB          */
+    uint32_t refill_free_percent; /* refill only when at least this share of the pool is free
+                                     (new paths then start together, as one wave); 0: always   */
+    uint32_t reserved;
 } cr_engine_tuning;
 
 typedef struct cr_engine_stats {
@@ -418,8 +425,8 @@ typedef struct cr_engine_stats {
 cr_status cr_gpu_render_batch(cr_job* jobs, uint32_t count, const cr_engine_tuning* tuning,
                               cr_engine_stats* stats);
 
-/* Picks pool size, refill interval and iterations per step for a batch by timing short trial
- * renders (the jobs at 1 sample per pixel) of candidate settings. The jobs are not modified. */
+/* Picks pool size and refill threshold for a batch by timing short trial renders (the jobs
+ * at 1 sample per pixel) of candidate settings. The jobs are not modified. */
 cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tuning* tuning);
 
 /* Continuous batching: a server owns an engine thread on `device`. Jobs submitted while

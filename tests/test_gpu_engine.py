@@ -62,6 +62,8 @@ def _alone(spec):
     None,
     dict(pool_paths=4096, range_samples=3000, refill_interval=1, iterations_per_step=4),
     dict(pool_paths=20000, range_samples=1 << 14, refill_interval=3, iterations_per_step=6, use_graphs=0),
+    dict(pool_paths=8192, range_samples=2000, issue_policy=2),
+    dict(pool_paths=8192, range_samples=5000, refill_free_percent=90),
 ])
 def test_batch_films_equal_single_renders(crgpu, world, tuning):
     jobs = _mixed_jobs(crgpu, world)
@@ -103,7 +105,7 @@ def test_batch_failures_stay_with_their_jobs(crgpu, world):
     bad_opts = JobSpec(world["room"], world["room_cam"], crgpu.Options.make(width=0, height=4, samples=1))
     jobs = [good, failing, invalid, bad_opts]
     stats = render_batch(jobs)
-    assert stats["jobs_done"] == 1 and stats["jobs_failed"] == 3
+    assert stats["jobs_done"] == 1 and stats["jobs_failed"] == 3, [(j.status, j.error) for j in jobs]
     film, _ = _alone(good)
     assert good.status == 0 and np.array_equal(good.film, film)
     for j in (failing, invalid, bad_opts):
@@ -166,8 +168,7 @@ def test_server_wait_timeout_and_budget(crgpu, world):
 def test_autotune_picks_a_measured_setting(crgpu, world):
     jobs = _mixed_jobs(crgpu, world)
     t = autotune_batch(jobs)
-    assert t.pool_paths in (1 << 22, 1 << 23, 1 << 24) and t.refill_interval in (1, 2, 4)
-    assert t.iterations_per_step % t.refill_interval == 0
+    assert t.pool_paths in (1 << 22, 1 << 24) and t.refill_free_percent in (0, 50, 90)
     stats = render_batch(jobs, t)
     assert stats["jobs_done"] == len(jobs)
     for j in jobs:

@@ -209,6 +209,7 @@ def _load():
         "cr_gpu_encode": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, P, C.c_uint64, C.POINTER(C.c_uint64)]),
         "cr_gpu_render_progressive": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.c_uint32, C.c_int, C.c_float,
                                                 FRAME_FN, P, P, C.POINTER(Stats), C.POINTER(Tuning)]),
+        "cr_gpu_phase_benchmark": (C.c_int, [P, C.POINTER(Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint64, P]),
         "cr_gpu_render_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning), C.POINTER(EngineStats)]),
         "cr_gpu_autotune_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning)]),
         "cr_server_create": (C.c_int, [C.c_int, C.POINTER(EngineTuning), C.POINTER(P)]),
@@ -424,6 +425,18 @@ class GpuScene:
         check(lib.cr_gpu_render_progressive(self.handle, C.byref(camera), C.byref(options), every, fmt, exposure, cb, None,
                                             film.ctypes.data, C.byref(stats), C.byref(tuning) if tuning else None))
         return frames, film, stats.as_dict()
+
+
+PHASES = ("camera", "closest-hit traversal", "occlusion traversal", "surface shading/maps", "BSDF sampling",
+          "BSDF evaluation", "HDR importance sample+lookup+PDF")
+phase_dtype = np.dtype([("seconds", "<f8"), ("calls", "<u8"), ("checksum", "<f8")])
+
+
+def phase_benchmark(scene, camera, width=320, height=180, count=400000, seed=42):
+    """cr_gpu_phase_benchmark: {phase: (seconds, calls, checksum)} in tests/benchmark.cpp's order."""
+    out = np.zeros(len(PHASES), phase_dtype)
+    check(lib.cr_gpu_phase_benchmark(scene.handle, C.byref(camera), width, height, count, seed, out.ctypes.data))
+    return {name: (float(r["seconds"]), int(r["calls"]), float(r["checksum"])) for name, r in zip(PHASES, out)}
 
 
 def display_thresholds(exposure=0.0):

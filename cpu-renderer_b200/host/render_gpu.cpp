@@ -22,6 +22,7 @@
 // exempt from access checks), so the reference's headers stay unmodified.
 #include "render.h"
 #include "cr_gpu.h"
+#include "render_gpu.h"
 
 #include <algorithm>
 #include <chrono>
@@ -163,10 +164,8 @@ struct SceneGuard {
 };
 }  // namespace
 
-// ---- render (render.cpp:352-456) ----------------------------------------------------------------
-RenderResult render(const Scene& scene, const Bvh& bvh, const Camera& camera, const Environment& environment,
-                    const RenderOptions& options, Progress progress) {
-    options.validate();
+// ---- scene upload (shared with the drop-in phase benchmark) ---------------------------------------
+cr_gpu_scene* uploadToGpu(const Scene& scene, const Bvh& bvh, const Environment& environment, int device) {
     // Scene arrays: triangles are binary-compatible; materials lose their names.
     std::vector<cr_material> materials(scene.materials.size());
     for (std::size_t i = 0; i < materials.size(); ++i) {
@@ -232,9 +231,19 @@ RenderResult render(const Scene& scene, const Bvh& bvh, const Camera& camera, co
     e.rotation_radians = environment.*get(EnvRotation{});
     e.intensity = environment.*get(EnvIntensity{});
 
-    SceneGuard g;
-    cr_status st = cr_gpu_scene_create(&d, &e, 0, &g.s);
+    cr_gpu_scene* handle = nullptr;
+    const cr_status st = cr_gpu_scene_create(&d, &e, device, &handle);
     if (st != CR_OK) raise(st);
+    return handle;
+}
+
+// ---- render (render.cpp:352-456) ----------------------------------------------------------------
+RenderResult render(const Scene& scene, const Bvh& bvh, const Camera& camera, const Environment& environment,
+                    const RenderOptions& options, Progress progress) {
+    options.validate();
+    SceneGuard g;
+    g.s = uploadToGpu(scene, bvh, environment, 0);
+    cr_status st = CR_OK;
     cr_camera c{};
     std::memcpy(c.position, &camera.position, 12); std::memcpy(c.forward, &camera.forward, 12);
     std::memcpy(c.right, &camera.right, 12); std::memcpy(c.up, &camera.up, 12);

@@ -368,6 +368,27 @@ cr_status cr_gpu_render_progressive(cr_gpu_scene* scene, const cr_camera* camera
                                     float* film_rgb, cr_render_stats* stats,
                                     const cr_gpu_tuning* tuning);
 
+/* ---- phase benchmark -----------------------------------------------------------------------
+ * tests/benchmark.cpp:18-62 on the device: camera (count rays at raster positions drawn from
+ * Rng(seed) for a width x height image, the reference's rays), closest-hit and occlusion
+ * traversal of those rays, surfaceAt for every hit, BSDF sampling and evaluation at every hit,
+ * environment sample + radiance + pdf (count calls; the scene's own environment). Each phase
+ * is one kernel over all its calls, run once untimed and once timed with CUDA events.
+ * out[CR_PHASE_*] receive seconds, calls and the reference's checksum term of each phase
+ * (hit t for closest hit, 1 per blocked ray for occlusion, pdfs for the BSDF phases,
+ * luminance + pdf for the environment; 0 for camera and surface). The BSDF and environment
+ * phases draw call i from its own stream Rng(sampleSeed(seed, i, phase)), where the
+ * reference continues one sequential stream. */
+enum { CR_PHASE_CAMERA = 0, CR_PHASE_CLOSEST_HIT, CR_PHASE_OCCLUSION, CR_PHASE_SURFACE, CR_PHASE_BSDF_SAMPLE,
+       CR_PHASE_BSDF_EVAL, CR_PHASE_ENVIRONMENT, CR_PHASE_COUNT };
+typedef struct cr_phase_timing {
+    double seconds;
+    uint64_t calls;
+    double checksum;
+} cr_phase_timing;
+cr_status cr_gpu_phase_benchmark(cr_gpu_scene* scene, const cr_camera* camera, int32_t width, int32_t height,
+                                 uint32_t count, uint64_t seed, cr_phase_timing* out);
+
 /* ---- many renders in one path pool ------------------------------------------------------------
  * No counterpart in the reference, which renders one image per cr::render call. The engine
  * runs the paths of many jobs (scene, camera, options) in one shared pool on one device: free

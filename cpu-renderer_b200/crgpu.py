@@ -209,6 +209,14 @@ def _load():
         "cr_gpu_encode": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, P, C.c_uint64, C.POINTER(C.c_uint64)]),
         "cr_gpu_render_progressive": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), C.c_uint32, C.c_int, C.c_float,
                                                 FRAME_FN, P, P, C.POINTER(Stats), C.POINTER(Tuning)]),
+        "cr_guide_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(P)]),
+        "cr_guide_destroy": (C.c_int, [P]),
+        "cr_guide_parameter_count": (C.c_uint32, []),
+        "cr_guide_get_parameters": (C.c_int, [P, P]),
+        "cr_guide_set_parameters": (C.c_int, [P, P]),
+        "cr_guide_evaluate": (C.c_int, [P, P, C.c_uint64, P]),
+        "cr_guide_gradients": (C.c_int, [P, P, C.c_uint64, P, C.POINTER(C.c_double)]),
+        "cr_guide_train": (C.c_int, [P, P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_float)]),
         "cr_gpu_phase_benchmark": (C.c_int, [P, C.POINTER(Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint64, P]),
         "cr_gpu_render_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning), C.POINTER(EngineStats)]),
         "cr_gpu_autotune_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning)]),
@@ -573,6 +581,56 @@ class Server:
             lib.cr_server_destroy(self.handle)
             self.handle = None
             self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Guide:
+    """cr_guide: the path-guiding network on a device."""
+
+    def __init__(self, device=0, seed=1):
+        h = C.c_void_p()
+        check(lib.cr_guide_create(device, seed, C.byref(h)))
+        self.handle = h
+        self.count = lib.cr_guide_parameter_count()
+
+    def parameters(self):
+        out = np.zeros(self.count, np.float32)
+        check(lib.cr_guide_get_parameters(self.handle, out.ctypes.data))
+        return out
+
+    def set_parameters(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.count
+        check(lib.cr_guide_set_parameters(self.handle, p.ctypes.data))
+
+    def evaluate(self, features):
+        f = np.ascontiguousarray(features, np.float32).reshape(-1, 9)
+        out = np.zeros((len(f), 40), np.float32)
+        check(lib.cr_guide_evaluate(self.handle, f.ctypes.data, len(f), out.ctypes.data))
+        return out
+
+    def gradients(self, samples):
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 13)
+        g = np.zeros(self.count, np.float32)
+        loss = C.c_double(0)
+        check(lib.cr_guide_gradients(self.handle, s.ctypes.data, len(s), g.ctypes.data, C.byref(loss)))
+        return g, loss.value
+
+    def train(self, samples, steps, batch=4096, lr=1e-3):
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 13)
+        loss = C.c_float(0)
+        check(lib.cr_guide_train(self.handle, s.ctypes.data, len(s), steps, batch, lr, C.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if self.handle:
+            lib.cr_guide_destroy(self.handle)
+            self.handle = None
 
     def __del__(self):
         try:

@@ -1,0 +1,570 @@
+// The path-guiding network on the device: inference on the tensor cores, training (forward,
+// backward, Adam) on the CUDA cores, and the cr_guide C ABI.
+//
+// Inference (k_guide_infer): one warp evaluates 32 rows. Activations live in shared memory as
+// FP16 (row stride 72 halves), weights as FP16 [out][in] (same stride); every layer is
+// mma.sync.m16n8k16 (FP16 x FP16 -> FP32) over 2 row tiles x (out / 8) column tiles x 4 k steps,
+// then bias + ReLU in FP32 and the result rounded back to FP16 for the next layer. The last
+// layer's 40 outputs are written as FP32.
+//
+// Training (k_guide_grad): one thread per sample computes the forward pass in FP32 with the
+// FP16-rounded weights (the values inference uses), the gradient of the weighted negative
+// log-likelihood  -w log q(dir)  with respect to the 40 outputs, and back-propagates. Weight
+// gradients of a block's 128 samples are summed in shared memory (activations and deltas of
+// all samples staged there) and added to the global gradient once per block. k_guide_adam
+// applies Adam (lr, beta1 0.9, beta2 0.999, eps 1e-8) to the FP32 masters and refreshes the
+// FP16 copy.
+#include "cr_guide.cuh"
+#include "cr_driver.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <vector>
+
+using namespace crg;
+using namespace crd;
+
+namespace crg {
+
+constexpr int kActStride = 72;  // halves per shared-memory row (64 + 8 against bank conflicts)
+constexpr int kInferWarps = 4;
+constexpr int kWeightRows = 3 * kGuideWidth + kGuideOutPad;  // 240 rows of 64 inputs
+
+struct GuideNetDev {
+    const __half* w16;  // [kGParams] FP16 copy (weights then biases)
+    const float* w32;   // [kGParams] FP16-rounded values as FP32 (training forward)
+};
+
+__device__ __forceinline__ uint32_t pack2(const __half* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__device__ __forceinline__ void mma16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// One dense layer for the warp's 32 rows: act (32 x 64, FP16) times W^T (W: [N][64] FP16).
+// N is 64 (hidden) or kGuideOutPad; outputs go back to act (FP16, after ReLU) or to out32.
+template <int N, bool LAST>
+__device__ void warpLayer(const __half* W, const float* bias, __half* act, float* out32) {
+    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    float acc[2][N / 8][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < N / 8; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = acc[mt][nt][2] = acc[mt][nt][3] = 0.0f;
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+        const int k0 = kt * 16 + tig * 2;
+        uint32_t a[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const __half* r0 = act + (mt * 16 + gid) * kActStride;
+            const __half* r1 = r0 + 8 * kActStride;
+            a[mt][0] = pack2(r0 + k0);
+            a[mt][1] = pack2(r1 + k0);
+            a[mt][2] = pack2(r0 + k0 + 8);
+            a[mt][3] = pack2(r1 + k0 + 8);
+        }
+#pragma unroll
+        for (int nt = 0; nt < N / 8; ++nt) {
+            const __half* wr = W + (nt * 8 + gid) * kActStride;
+            const uint32_t b0 = pack2(wr + k0), b1 = pack2(wr + k0 + 8);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) mma16816(acc[mt][nt], a[mt][0], a[mt][1], a[mt][2], a[mt][3], b0, b1);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < N / 8; ++nt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {  // h = 0: row gid, h = 1: row gid + 8
+                const int row = mt * 16 + gid + 8 * h, col = nt * 8 + tig * 2;
+                float v0 = acc[mt][nt][2 * h] + bias[col], v1 = acc[mt][nt][2 * h + 1] + bias[col + 1];
+                if (LAST) {
+                    if (col < kGuideOut) out32[row * kGuideOut + col] = v0;
+                    if (col + 1 < kGuideOut) out32[row * kGuideOut + col + 1] = v1;
+                } else {
+                    v0 = fmaxf(v0, 0.0f);
+                    v1 = fmaxf(v1, 0.0f);
+                    act[row * kActStride + col] = __float2half_rn(v0);
+                    act[row * kActStride + col + 1] = __float2half_rn(v1);
+                }
+            }
+    __syncwarp();
+}
+
+// Loads the FP16 weights (row stride kActStride) and FP32 biases into shared memory.
+__device__ void loadNet(const GuideNetDev& net, __half* sW, float* sB) {
+    for (int i = threadIdx.x; i < kWeightRows * kGuideIn; i += blockDim.x) {
+        const int r = i / kGuideIn, c = i % kGuideIn;
+        sW[r * kActStride + c] = net.w16[r * kGuideIn + c];
+    }
+    for (int i = threadIdx.x; i < kGParams - kGWCount; i += blockDim.x) sB[i] = __half2float(net.w16[kGWCount + i]);
+    __syncthreads();
+}
+
+// Row i's features: from an explicit array (features != nullptr) or from a traced path.
+struct InferRows {
+    const float* features;       // [n][9], or nullptr
+    const uint32_t* queue;       // path indices (when features == nullptr)
+    const uint32_t* queueCount;  // device count of the queue
+    uint64_t n;                  // rows when features != nullptr
+    // path inputs
+    const float4* rayO;
+    const float4* rayD;
+    const float* hitT;
+    const uint32_t* hitTri;
+    const float4* triNg;
+    V3 lo, inv;
+    float* out;                  // [row or path][kGuideOut]
+};
+
+__device__ bool rowFeatures(const InferRows& R, uint64_t i, float f[kGuideFeatures], uint64_t& outRow) {
+    if (R.features) {
+        for (int k = 0; k < kGuideFeatures; ++k) f[k] = R.features[i * kGuideFeatures + k];
+        outRow = i;
+        return true;
+    }
+    const uint32_t path = R.queue[i];
+    outRow = path;
+    const uint32_t tri = R.hitTri[path];
+    if (tri == kNoTriangle) return false;
+    const float4 o = R.rayO[path], d = R.rayD[path];
+    const float t = R.hitT[path];
+    const V3 p{o.x + t * d.x, o.y + t * d.y, o.z + t * d.z};
+    const float4 ng = R.triNg[tri];
+    f[0] = (p.x - R.lo.x) * R.inv.x; f[1] = (p.y - R.lo.y) * R.inv.y; f[2] = (p.z - R.lo.z) * R.inv.z;
+    f[3] = -d.x; f[4] = -d.y; f[5] = -d.z;
+    f[6] = ng.x; f[7] = ng.y; f[8] = ng.z;
+    return true;
+}
+
+__global__ void __launch_bounds__(32 * kInferWarps) k_guide_infer(GuideNetDev net, InferRows R) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __half* sW = reinterpret_cast<__half*>(smem);
+    float* sB = reinterpret_cast<float*>(sW + kWeightRows * kActStride);
+    __half* sAct = reinterpret_cast<__half*>(sB + (kGParams - kGWCount));
+    float* sOut = reinterpret_cast<float*>(sAct + kInferWarps * 32 * kActStride);
+    loadNet(net, sW, sB);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __half* act = sAct + warp * 32 * kActStride;
+    float* out = sOut + warp * 32 * kGuideOut;
+    const uint64_t rows = R.features ? R.n : *R.queueCount;
+    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(kInferWarps) + warp) * 32; base < rows;
+         base += static_cast<uint64_t>(gridDim.x) * kInferWarps * 32) {
+        const uint64_t i = base + lane;
+        float f[kGuideFeatures] = {};
+        uint64_t outRow = 0;
+        const bool valid = i < rows && rowFeatures(R, i, f, outRow);
+        float x[kGuideIn];
+        guideEncode(f, x);
+        for (int c = 0; c < kGuideIn; ++c) act[lane * kActStride + c] = __float2half_rn(valid ? x[c] : 0.0f);
+        __syncwarp();
+        warpLayer<kGuideWidth, false>(sW + kGW1 / kGuideIn * kActStride, sB + (kGB1 - kGWCount), act, nullptr);
+        warpLayer<kGuideWidth, false>(sW + kGW2 / kGuideIn * kActStride, sB + (kGB2 - kGWCount), act, nullptr);
+        warpLayer<kGuideWidth, false>(sW + kGW3 / kGuideIn * kActStride, sB + (kGB3 - kGWCount), act, nullptr);
+        warpLayer<kGuideOutPad, true>(sW + kGW4 / kGuideIn * kActStride, sB + (kGB4 - kGWCount), act, out);
+        if (valid)
+            for (int c = 0; c < kGuideOut; ++c) R.out[outRow * kGuideOut + c] = out[lane * kGuideOut + c];
+        __syncwarp();
+    }
+}
+
+// d(-log q(dir))/d(outputs) for one sample; returns -log q.
+__device__ float mixtureGrad(const float* out, V3 dir, float* g) {
+    float lp[kGuideLobes], lf[kGuideLobes], mxl = -1e30f;
+    float kap[kGuideLobes], mlen[kGuideLobes], cosv[kGuideLobes];
+    V3 mu[kGuideLobes];
+    for (int j = 0; j < kGuideLobes; ++j) mxl = fmaxf(mxl, out[5 * j]);
+    float zs = 0;
+    for (int j = 0; j < kGuideLobes; ++j) zs += expf(out[5 * j] - mxl);
+    const float logZ = mxl + logf(zs);
+    float mx = -1e30f;
+    for (int j = 0; j < kGuideLobes; ++j) {
+        lp[j] = out[5 * j] - logZ;  // log pi_j
+        const float lk = fminf(fmaxf(out[5 * j + 1], kLogKappaMin), kLogKappaMax);
+        kap[j] = expf(lk);
+        const V3 raw{out[5 * j + 2], out[5 * j + 3], out[5 * j + 4]};
+        mlen[j] = sqrtf(dot(raw, raw));
+        mu[j] = mlen[j] > 1e-12f ? raw * (1.0f / mlen[j]) : V3{0, 0, 1};
+        cosv[j] = dot(mu[j], dir);
+        lf[j] = lp[j] + vmfLogPdf(mu[j], kap[j], dir);
+        mx = fmaxf(mx, lf[j]);
+    }
+    float s = 0;
+    for (int j = 0; j < kGuideLobes; ++j) s += expf(lf[j] - mx);
+    const float logq = mx + logf(s);
+    for (int j = 0; j < kGuideLobes; ++j) {
+        const float r = expf(lf[j] - logq), pi = expf(lp[j]);
+        g[5 * j] = pi - r;
+        const float lk = out[5 * j + 1];
+        const float k = kap[j];
+        // d log vMF / d log k = 1 - 2k / (e^2k - 1) + k (c - 1)
+        const float dlk = 1 - (k > 1e-4f ? 2 * k / expm1f(2 * k) : 1.0f) + k * (cosv[j] - 1);
+        g[5 * j + 1] = (lk > kLogKappaMin && lk < kLogKappaMax) ? -r * dlk : 0.0f;
+        const float sc = mlen[j] > 1e-12f ? -r * k / mlen[j] : 0.0f;  // d/dm = -r k (dir - c mu) / |m|
+        g[5 * j + 2] = sc * (dir.x - cosv[j] * mu[j].x);
+        g[5 * j + 3] = sc * (dir.y - cosv[j] * mu[j].y);
+        g[5 * j + 4] = sc * (dir.z - cosv[j] * mu[j].z);
+    }
+    return -logq;
+}
+
+constexpr int kTrainThreads = 128;
+
+// Block-summed outer products: grad[W + n*IN + k] += sum_t D[t][n] * H[t][k], grad[B + n] += sum_t D[t][n].
+template <int NOUT, int NIN>
+__device__ void accumulateLayer(const float* D, const float* H, float* grad, int wOff, int bOff) {
+    for (int e = threadIdx.x; e < NOUT * NIN; e += blockDim.x) {
+        const int n = e / NIN, k = e % NIN;
+        float acc = 0;
+        for (int t = 0; t < kTrainThreads; ++t) acc += D[t * (kGuideWidth + 1) + n] * H[t * (kGuideWidth + 1) + k];
+        if (acc != 0.0f) atomicAdd(&grad[wOff + n * kGuideIn + k], acc);
+    }
+    for (int n = threadIdx.x; n < NOUT; n += blockDim.x) {
+        float acc = 0;
+        for (int t = 0; t < kTrainThreads; ++t) acc += D[t * (kGuideWidth + 1) + n];
+        if (acc != 0.0f) atomicAdd(&grad[bOff + n], acc);
+    }
+}
+
+// samples: [n][13] = features (9), dir (3), weight. grad += d(sum_i scale * w_i * -log q_i).
+__global__ void __launch_bounds__(kTrainThreads) k_guide_grad(GuideNetDev net, const GuideSample* samples, uint64_t n,
+                                                              float scale, float* grad, double* loss) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* sP = reinterpret_cast<float*>(smem);                    // kGParams
+    float* sH = sP + kGParams;                                     // [128][65] layer input
+    float* sD = sH + kTrainThreads * (kGuideWidth + 1);            // [128][65] layer delta
+    for (int i = threadIdx.x; i < kGParams; i += blockDim.x) sP[i] = net.w32[i];
+    __syncthreads();
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(kTrainThreads) + threadIdx.x;
+    const bool valid = i < n;
+    float f[kGuideFeatures] = {};
+    V3 dir{0, 0, 1};
+    float w = 0;
+    if (valid) {
+        const GuideSample smp = samples[i];
+        for (int k = 0; k < kGuideFeatures; ++k) f[k] = smp.feat[k];
+        dir = V3{smp.dir[0], smp.dir[1], smp.dir[2]};
+        w = smp.weight * scale;
+    }
+    float x[kGuideIn], h1[kGuideWidth], h2[kGuideWidth], h3[kGuideWidth], o[kGuideOutPad];
+    guideEncode(f, x);
+    auto dense = [&](const float* in, float* outv, int wOff, int bOff, int nout, bool relu) {
+        for (int r = 0; r < nout; ++r) {
+            float a = sP[bOff + r];
+            const float* wr = sP + wOff + r * kGuideIn;
+            for (int k = 0; k < kGuideIn; ++k) a += wr[k] * in[k];
+            outv[r] = relu ? fmaxf(a, 0.0f) : a;
+        }
+    };
+    dense(x, h1, kGW1, kGB1, kGuideWidth, true);
+    dense(h1, h2, kGW2, kGB2, kGuideWidth, true);
+    dense(h2, h3, kGW3, kGB3, kGuideWidth, true);
+    dense(h3, o, kGW4, kGB4, kGuideOutPad, false);
+    float g[kGuideOutPad];
+    for (int k = 0; k < kGuideOutPad; ++k) g[k] = 0;
+    float nll = 0;
+    if (valid && w > 0) {
+        nll = mixtureGrad(o, dir, g);
+        for (int k = 0; k < kGuideOut; ++k) g[k] *= w;
+    }
+    if (valid) atomicAdd(loss, static_cast<double>(w * nll));
+    float* myH = sH + threadIdx.x * (kGuideWidth + 1);
+    float* myD = sD + threadIdx.x * (kGuideWidth + 1);
+    // layer 4: delta = g (48), input h3
+    for (int k = 0; k < kGuideWidth; ++k) myH[k] = h3[k];
+    for (int k = 0; k < kGuideOutPad; ++k) myD[k] = g[k];
+    __syncthreads();
+    accumulateLayer<kGuideOutPad, kGuideWidth>(sD, sH, grad, kGW4, kGB4);
+    __syncthreads();
+    float d[kGuideWidth];
+    auto backLayer = [&](const float* delta, int nout, int wOff, const float* act, float* dIn) {
+        for (int k = 0; k < kGuideWidth; ++k) {
+            float a = 0;
+            for (int r = 0; r < nout; ++r) a += sP[wOff + r * kGuideIn + k] * delta[r];
+            dIn[k] = act[k] > 0 ? a : 0.0f;  // through the ReLU of the layer that made act
+        }
+    };
+    backLayer(g, kGuideOutPad, kGW4, h3, d);
+    for (int k = 0; k < kGuideWidth; ++k) { myH[k] = h2[k]; myD[k] = d[k]; }
+    __syncthreads();
+    accumulateLayer<kGuideWidth, kGuideWidth>(sD, sH, grad, kGW3, kGB3);
+    __syncthreads();
+    float d2[kGuideWidth];
+    backLayer(d, kGuideWidth, kGW3, h2, d2);
+    for (int k = 0; k < kGuideWidth; ++k) { myH[k] = h1[k]; myD[k] = d2[k]; }
+    __syncthreads();
+    accumulateLayer<kGuideWidth, kGuideWidth>(sD, sH, grad, kGW2, kGB2);
+    __syncthreads();
+    backLayer(d2, kGuideWidth, kGW2, h1, d);
+    for (int k = 0; k < kGuideWidth; ++k) { myH[k] = x[k]; myD[k] = d[k]; }
+    __syncthreads();
+    accumulateLayer<kGuideWidth, kGuideIn>(sD, sH, grad, kGW1, kGB1);
+}
+
+__global__ void k_guide_adam(float* p, float* g, float* m, float* v, __half* p16, float* p32, int count, float lr,
+                             float bc1, float bc2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = 0.9f * m[i] + 0.1f * gi, vi = 0.999f * v[i] + 0.001f * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
+        p[i] = pi;
+        const __half h = __float2half_rn(pi);
+        p16[i] = h;
+        p32[i] = __half2float(h);
+        g[i] = 0.0f;
+    }
+}
+
+__global__ void k_guide_refresh(const float* p, __half* p16, float* p32, int count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const __half h = __float2half_rn(p[i]);
+        p16[i] = h;
+        p32[i] = __half2float(h);
+    }
+}
+
+constexpr size_t kInferSmem = kWeightRows * kActStride * sizeof(__half) + (kGParams - kGWCount) * sizeof(float) +
+                              kInferWarps * 32 * kActStride * sizeof(__half) + kInferWarps * 32 * kGuideOut * sizeof(float);
+constexpr size_t kTrainSmem = kGParams * sizeof(float) + 2 * kTrainThreads * (kGuideWidth + 1) * sizeof(float);
+
+}  // namespace crg
+
+struct cr_guide {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevAlloc mem;
+    float* p = nullptr;    // FP32 masters
+    float* g = nullptr;    // gradient
+    float* m = nullptr;
+    float* v = nullptr;
+    __half* p16 = nullptr;
+    float* p32 = nullptr;  // FP16-rounded values as FP32
+    double* loss = nullptr;
+    uint64_t step = 0;
+    int inferGrid = 0;
+    DevAlloc scratch;      // caller data for the test entry points
+    size_t scratchBytes = 0;
+    void* scratchPtr = nullptr;
+
+    GuideNetDev net() const { return GuideNetDev{p16, p32}; }
+    void* ensureScratch(size_t bytes) {
+        if (bytes > scratchBytes) {
+            scratch.release();
+            scratchPtr = scratch.alloc<unsigned char>(bytes);
+            scratchBytes = bytes;
+        }
+        return scratchPtr;
+    }
+    ~cr_guide() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        mem.release();
+        scratch.release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace crg {
+
+void guideAttributes() {
+    static bool done = false;
+    if (done) return;
+    CR_CUDA(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kInferSmem)));
+    CR_CUDA(cudaFuncSetAttribute(k_guide_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTrainSmem)));
+    done = true;
+}
+
+// Inference over a traced path queue (guided renders): out[path][40] for the paths of `queue`.
+void guideInferPaths(cr_guide* gd, cudaStream_t s, const uint32_t* queue, const uint32_t* queueCount, uint32_t maxRows,
+                     const PathSoA& st, const float* hitT, const DevScene& S, V3 lo, V3 inv, float* out) {
+    guideAttributes();
+    InferRows R{};
+    R.queue = queue; R.queueCount = queueCount;
+    R.rayO = st.ray_o; R.rayD = st.ray_d; R.hitT = hitT; R.hitTri = st.hit_tri; R.triNg = S.tri_ng;
+    R.lo = lo; R.inv = inv; R.out = out;
+    const uint32_t rowsPerBlock = 32 * kInferWarps;
+    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(static_cast<uint32_t>(gd->inferGrid),
+                                                                     (maxRows + rowsPerBlock - 1) / rowsPerBlock));
+    k_guide_infer<<<blocks, 32 * kInferWarps, kInferSmem, s>>>(gd->net(), R);
+    CR_CUDA(cudaGetLastError());
+}
+
+// Adam steps on device-resident samples: `steps` mini-batches of `batch` consecutive samples
+// (wrapping around), loss weights normalised by the collection's mean weight.
+float guideTrain(cr_guide* gd, cudaStream_t s, const GuideSample* samples, uint64_t n, uint32_t steps, uint32_t batch,
+                 float lr, double weightMean) {
+    guideAttributes();
+    if (n == 0 || steps == 0) return 0.0f;
+    const uint64_t b = std::min<uint64_t>(batch, n);
+    const float scale = static_cast<float>(1.0 / (static_cast<double>(b) * (weightMean > 0 ? weightMean : 1.0)));
+    double lossHost = 0;
+    uint64_t at = 0;
+    for (uint32_t k = 0; k < steps; ++k) {
+        const uint64_t count = std::min<uint64_t>(b, n - at);
+        CR_CUDA(cudaMemsetAsync(gd->loss, 0, sizeof(double), s));
+        k_guide_grad<<<static_cast<unsigned>((count + kTrainThreads - 1) / kTrainThreads), kTrainThreads, kTrainSmem, s>>>(
+            gd->net(), samples + at, count, scale, gd->g, gd->loss);
+        ++gd->step;
+        const float bc1 = 1.0f - std::pow(0.9f, static_cast<float>(gd->step));
+        const float bc2 = 1.0f - std::pow(0.999f, static_cast<float>(gd->step));
+        k_guide_adam<<<64, 256, 0, s>>>(gd->p, gd->g, gd->m, gd->v, gd->p16, gd->p32, kGParams, lr, bc1, bc2);
+        CR_CUDA(cudaGetLastError());
+        at = (at + count) % n;
+    }
+    CR_CUDA(cudaMemcpyAsync(&lossHost, gd->loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CR_CUDA(cudaStreamSynchronize(s));
+    return static_cast<float>(lossHost);
+}
+
+}  // namespace crg
+
+extern "C" {
+
+uint32_t cr_guide_parameter_count(void) { return kGParams; }
+
+cr_status cr_guide_create(int device, uint64_t seed, cr_guide** out) {
+    try {
+        if (!out) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        CR_CUDA(cudaSetDevice(device));
+        auto gd = std::make_unique<cr_guide>();
+        gd->device = device;
+        CR_CUDA(cudaStreamCreateWithFlags(&gd->stream, cudaStreamNonBlocking));
+        gd->p = gd->mem.alloc<float>(kGParams);
+        gd->g = gd->mem.alloc<float>(kGParams);
+        gd->m = gd->mem.alloc<float>(kGParams);
+        gd->v = gd->mem.alloc<float>(kGParams);
+        gd->p16 = gd->mem.alloc<__half>(kGParams);
+        gd->p32 = gd->mem.alloc<float>(kGParams);
+        gd->loss = gd->mem.alloc<double>(1);
+        // He-uniform hidden layers, a small output layer: lobes start broad (kappa 1), equally
+        // weighted, with means along seeded random directions.
+        std::vector<float> h(kGParams, 0.0f);
+        std::mt19937_64 rng(seed);
+        std::uniform_real_distribution<float> uni(-1.0f, 1.0f);
+        const float lim = std::sqrt(6.0f / kGuideIn);
+        for (int i = kGW1; i < kGW4; ++i) h[i] = lim * uni(rng);
+        for (int r = 0; r < kGuideOut; ++r)
+            for (int k = 0; k < kGuideIn; ++k) h[kGW4 + r * kGuideIn + k] = 1e-3f * uni(rng);
+        for (int j = 0; j < kGuideLobes; ++j) {
+            std::normal_distribution<float> nd;
+            float a = nd(rng), b = nd(rng), c = nd(rng);
+            const float l = std::sqrt(a * a + b * b + c * c) + 1e-12f;
+            h[kGB4 + 5 * j + 2] = a / l; h[kGB4 + 5 * j + 3] = b / l; h[kGB4 + 5 * j + 4] = c / l;
+        }
+        CR_CUDA(cudaMemcpyAsync(gd->p, h.data(), kGParams * sizeof(float), cudaMemcpyHostToDevice, gd->stream));
+        CR_CUDA(cudaMemsetAsync(gd->g, 0, kGParams * sizeof(float), gd->stream));
+        CR_CUDA(cudaMemsetAsync(gd->m, 0, kGParams * sizeof(float), gd->stream));
+        CR_CUDA(cudaMemsetAsync(gd->v, 0, kGParams * sizeof(float), gd->stream));
+        k_guide_refresh<<<64, 256, 0, gd->stream>>>(gd->p, gd->p16, gd->p32, kGParams);
+        CR_CUDA(cudaGetLastError());
+        CR_CUDA(cudaStreamSynchronize(gd->stream));
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        gd->inferGrid = sms * 2;
+        guideAttributes();
+        *out = gd.release();
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_guide_destroy(cr_guide* gd) {
+    delete gd;
+    return CR_OK;
+}
+
+cr_status cr_guide_get_parameters(cr_guide* gd, float* out) {
+    try {
+        if (!gd || !out) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        CR_CUDA(cudaSetDevice(gd->device));
+        CR_CUDA(cudaMemcpyAsync(out, gd->p, kGParams * sizeof(float), cudaMemcpyDeviceToHost, gd->stream));
+        CR_CUDA(cudaStreamSynchronize(gd->stream));
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_guide_set_parameters(cr_guide* gd, const float* in) {
+    try {
+        if (!gd || !in) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        CR_CUDA(cudaSetDevice(gd->device));
+        CR_CUDA(cudaMemcpyAsync(gd->p, in, kGParams * sizeof(float), cudaMemcpyHostToDevice, gd->stream));
+        k_guide_refresh<<<64, 256, 0, gd->stream>>>(gd->p, gd->p16, gd->p32, kGParams);
+        CR_CUDA(cudaGetLastError());
+        CR_CUDA(cudaStreamSynchronize(gd->stream));
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_guide_evaluate(cr_guide* gd, const float* features, uint64_t n, float* out) {
+    try {
+        if (!gd || !features || !out) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (n == 0) return CR_OK;
+        CR_CUDA(cudaSetDevice(gd->device));
+        const size_t inBytes = n * kGuideFeatures * sizeof(float), outBytes = n * kGuideOut * sizeof(float);
+        unsigned char* buf = static_cast<unsigned char*>(gd->ensureScratch(inBytes + outBytes + 256));
+        float* dIn = reinterpret_cast<float*>(buf);
+        float* dOut = reinterpret_cast<float*>(buf + (inBytes + 255) / 256 * 256);
+        CR_CUDA(cudaMemcpyAsync(dIn, features, inBytes, cudaMemcpyHostToDevice, gd->stream));
+        InferRows R{};
+        R.features = dIn; R.n = n; R.out = dOut;
+        const uint64_t blocks = std::min<uint64_t>(static_cast<uint64_t>(gd->inferGrid), (n + 127) / 128);
+        k_guide_infer<<<static_cast<unsigned>(std::max<uint64_t>(1, blocks)), 32 * kInferWarps, kInferSmem, gd->stream>>>(gd->net(), R);
+        CR_CUDA(cudaGetLastError());
+        CR_CUDA(cudaMemcpyAsync(out, dOut, outBytes, cudaMemcpyDeviceToHost, gd->stream));
+        CR_CUDA(cudaStreamSynchronize(gd->stream));
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// samples: n x 13 floats (features 9, direction 3, weight). grad receives
+// d/dparams of sum_i w_i * -log q_i(dir_i); *loss that sum.
+cr_status cr_guide_gradients(cr_guide* gd, const float* samples, uint64_t n, float* grad, double* loss) {
+    try {
+        if (!gd || !samples || !grad || !loss) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        CR_CUDA(cudaSetDevice(gd->device));
+        static_assert(sizeof(GuideSample) == 13 * sizeof(float), "GuideSample is 13 floats");
+        GuideSample* d = static_cast<GuideSample*>(gd->ensureScratch(n * sizeof(GuideSample) + 16));
+        CR_CUDA(cudaMemcpyAsync(d, samples, n * sizeof(GuideSample), cudaMemcpyHostToDevice, gd->stream));
+        CR_CUDA(cudaMemsetAsync(gd->g, 0, kGParams * sizeof(float), gd->stream));
+        CR_CUDA(cudaMemsetAsync(gd->loss, 0, sizeof(double), gd->stream));
+        k_guide_grad<<<static_cast<unsigned>((n + kTrainThreads - 1) / kTrainThreads), kTrainThreads, kTrainSmem, gd->stream>>>(
+            gd->net(), d, n, 1.0f, gd->g, gd->loss);
+        CR_CUDA(cudaGetLastError());
+        CR_CUDA(cudaMemcpyAsync(grad, gd->g, kGParams * sizeof(float), cudaMemcpyDeviceToHost, gd->stream));
+        CR_CUDA(cudaMemcpyAsync(loss, gd->loss, sizeof(double), cudaMemcpyDeviceToHost, gd->stream));
+        CR_CUDA(cudaMemsetAsync(gd->g, 0, kGParams * sizeof(float), gd->stream));
+        CR_CUDA(cudaStreamSynchronize(gd->stream));
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// Adam on caller samples (host memory): `steps` mini-batches of `batch`; *loss receives the
+// last batch's normalised loss.
+cr_status cr_guide_train(cr_guide* gd, const float* samples, uint64_t n, uint32_t steps, uint32_t batch, float lr,
+                         float* loss) {
+    try {
+        if (!gd || !samples || n == 0) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        CR_CUDA(cudaSetDevice(gd->device));
+        GuideSample* d = static_cast<GuideSample*>(gd->ensureScratch(n * sizeof(GuideSample) + 16));
+        CR_CUDA(cudaMemcpyAsync(d, samples, n * sizeof(GuideSample), cudaMemcpyHostToDevice, gd->stream));
+        double mean = 0;
+        for (uint64_t i = 0; i < n; ++i) mean += samples[13 * i + 12];
+        mean /= static_cast<double>(n);
+        const float l = guideTrain(gd, gd->stream, d, n, steps, batch, lr, mean);
+        if (loss) *loss = l;
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+}  // extern "C"

@@ -389,6 +389,31 @@ typedef struct cr_phase_timing {
 cr_status cr_gpu_phase_benchmark(cr_gpu_scene* scene, const cr_camera* camera, int32_t width, int32_t height,
                                  uint32_t count, uint64_t seed, cr_phase_timing* out);
 
+/* ---- learned path guiding -----------------------------------------------------------------------
+ * No counterpart in the reference. A cr_guide is a small network on one device: 4 dense layers
+ * 64 wide map a shading point (position scaled to the scene bounds, outgoing direction,
+ * geometric normal; 9 features, encoded to 64 inputs) to a mixture of 8 von Mises-Fisher
+ * lobes (40 outputs: per lobe the mixture logit, log kappa and the unnormalised mean). Its
+ * weights are FP32 masters (trained by Adam) with an FP16 copy used by inference on the tensor
+ * cores (FP32 accumulation). cr_gpu_render_guided trains it online on the tracer's own radiance
+ * samples and samples directions from it, mixed with BSDF sampling by one-sample MIS. */
+typedef struct cr_guide cr_guide;
+cr_status cr_guide_create(int device, uint64_t seed, cr_guide** out);
+cr_status cr_guide_destroy(cr_guide* guide);
+uint32_t cr_guide_parameter_count(void);
+cr_status cr_guide_get_parameters(cr_guide* guide, float* out);       /* FP32 masters */
+cr_status cr_guide_set_parameters(cr_guide* guide, const float* in);  /* also refreshes the FP16 copy */
+/* features: n x 9 floats; out: n x 40 network outputs (tensor-core inference). */
+cr_status cr_guide_evaluate(cr_guide* guide, const float* features, uint64_t n, float* out);
+/* samples: n x 13 floats (features 9, direction 3, weight w). grad (parameter count floats)
+ * receives d/dparams of sum_i w_i * -log q_i(direction_i), *loss that sum, with the FP16-rounded
+ * weights inference uses. */
+cr_status cr_guide_gradients(cr_guide* guide, const float* samples, uint64_t n, float* grad, double* loss);
+/* `steps` Adam steps (learning rate lr) over mini-batches of `batch` of the samples, weights
+ * normalised by their mean; *loss receives the last batch's loss. */
+cr_status cr_guide_train(cr_guide* guide, const float* samples, uint64_t n, uint32_t steps, uint32_t batch, float lr,
+                         float* loss);
+
 /* ---- many renders in one path pool ------------------------------------------------------------
  * No counterpart in the reference, which renders one image per cr::render call. The engine
  * runs the paths of many jobs (scene, camera, options) in one shared pool on one device: free

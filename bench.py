@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-spp", type=int, default=4)
-    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "serve"],
+    ap.add_argument("--workload", default="grid", choices=["grid", "batch", "serve", "guided"],
                     help="grid: the 1M-triangle 1080p render (default); batch: 64 uneven scenes in one pool "
                          "against one by one; serve: a Poisson request stream through the server")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream (2000 for the full run)")
@@ -461,6 +461,97 @@ def run_serve(args):
         g.close()
 
 
+def _loglog(curve, x):
+    """A measured (x, y) curve interpolated in log-log at x; None outside its range."""
+    pts = sorted(curve)
+    for (x0, y0), (x1, y1) in zip(pts, pts[1:]):
+        if x0 <= x <= x1:
+            if x1 == x0:
+                return y0
+            a = (math.log(x) - math.log(x0)) / (math.log(x1) - math.log(x0))
+            return math.exp(math.log(y0) + a * (math.log(y1) - math.log(y0)))
+    return None
+
+
+def _time_to(curve, target):
+    """Seconds to reach relMSE `target` on a measured (seconds, relMSE) curve, interpolated in
+    log-log; None when the curve does not reach it (no extrapolation)."""
+    pts = sorted(curve)
+    for (t0, e0), (t1, e1) in zip(pts, pts[1:]):
+        if e0 >= target >= e1:
+            return _loglog([(e1, t1), (e0, t0)], target)
+    return None
+
+
+def run_guided(args):
+    """Learned proposal against the plain tracer: relative MSE (against a plain high-sample
+    reference) versus wall time, on the caustic sphere grid lit only by the sun disk and on the
+    room with next-event estimation off."""
+    import crgpu
+    import workloads
+
+    def curve(g, cam, make_opt, spps, guided):
+        out = []
+        for spp in spps:
+            gd = crgpu.Guide(seed=1) if guided else None
+            t0 = time.perf_counter()
+            if guided:
+                film, _ = g.render_guided(cam, make_opt(spp), gd, train_samples=min(32, spp))
+            else:
+                film, _ = g.render(cam, make_opt(spp))
+            sec = time.perf_counter() - t0
+            out.append((sec, spp, film))
+            if gd:
+                gd.close()
+        return out
+
+    results = {}
+    for name, sc, (w, h), bounces, nee, spps, ref_spp in (
+            ("caustic_sphere_grid", workloads.caustic_scene(320, 180), (320, 180), 16, True, (64, 256, 1024, 4096), 16384),
+            ("room_without_nee", workloads.room_scene(), (64, 64), 8, False, (256, 1024, 4096), 65536)):
+        tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
+        env = crgpu.env_desc(image=sc["env_image"]) if sc.get("env_image") is not None else None
+        g = crgpu.GpuScene(tris, sc["materials"], env=env)
+        cam = sc["camera"]
+        make_opt = lambda spp, seed=42: crgpu.Options.make(width=w, height=h, samples=spp, bounces=bounces, seed=seed, nee=nee)
+        g.render(cam, make_opt(4))  # warm-up
+        t0 = time.perf_counter()
+        ref, _ = g.render(cam, make_opt(ref_spp, seed=7))
+        ref_s = time.perf_counter() - t0
+        entry = {"width": w, "height": h, "bounces": bounces, "nee": nee, "reference_spp": ref_spp,
+                 "reference_seconds": ref_s}
+        curves = {}
+        for label, guided in (("plain", False), ("guided", True)):
+            c = curve(g, cam, make_opt, spps, guided)
+            pts = [(sec, crgpu.rel_mse(film, ref)) for sec, _, film in c]
+            curves[label] = pts
+            entry[label] = {"spp": list(spps), "seconds": [p[0] for p in pts], "rel_mse": [p[1] for p in pts],
+                            "mean": [float(f.mean()) for _, _, f in c],
+                            "seconds_to_rel_mse_1e-3": _time_to(pts, 1e-3)}
+        pt, gt = entry["plain"]["seconds_to_rel_mse_1e-3"], entry["guided"]["seconds_to_rel_mse_1e-3"]
+        entry["guided_over_plain_time_to_1e-3"] = gt / pt if pt and gt else None
+        entry["rel_mse_ratio_at_equal_spp"] = [gq / pq for gq, pq in zip(entry["guided"]["rel_mse"], entry["plain"]["rel_mse"])]
+        # guided error over the plain tracer's error after the same wall time (where measured)
+        equal_time = []
+        for t, e in curves["guided"]:
+            p = _loglog(curves["plain"], t)
+            equal_time.append(e / p if p else None)
+        entry["rel_mse_ratio_at_equal_time"] = equal_time
+        results[name] = entry
+        g.close()
+    c5 = results["caustic_sphere_grid"]
+    line = {
+        "metric": "time to relMSE 1e-3, guided / plain", "value": c5["guided_over_plain_time_to_1e-3"], "unit": "ratio",
+        "note": "null when either tracer does not reach relMSE 1e-3 within the measured samples (no extrapolation)",
+        "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 tracer, fp16 network (fp32 accumulation)", "data": "synthetic (seeded procedural scenes)",
+        "config": {"workload": "learned-proposal", "network": "4x64 MLP, 8 vMF lobes, Adam lr 1e-3, trained on the first 32 spp",
+                   "guide_probability": 0.5, "reference": "plain tracer, same scene, 16384 spp (room: 65536)"},
+        "scenes": results,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -469,6 +560,8 @@ def main():
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "guided":
+        run_guided(args)
     else:
         run_ours(args)
 

@@ -147,6 +147,11 @@ ENCODE_SRGB8, ENCODE_RGBE, ENCODE_HDR_FILE = 0, 1, 2
 FRAME_FN = C.CFUNCTYPE(None, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p)
 
 
+class GuideOptions(C.Structure):
+    _fields_ = [("train_samples", C.c_uint32), ("guide_probability", C.c_float), ("batch", C.c_uint32),
+                ("epochs", C.c_uint32)]
+
+
 class Job(C.Structure):
     """cr_job: one render of a batch or server."""
     _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("options", Options), ("film_rgb", C.c_void_p),
@@ -217,6 +222,8 @@ def _load():
         "cr_guide_evaluate": (C.c_int, [P, P, C.c_uint64, P]),
         "cr_guide_gradients": (C.c_int, [P, P, C.c_uint64, P, C.POINTER(C.c_double)]),
         "cr_guide_train": (C.c_int, [P, P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(C.c_float)]),
+        "cr_gpu_render_guided": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), P, C.POINTER(GuideOptions), P,
+                                           C.POINTER(Stats), C.POINTER(Tuning)]),
         "cr_gpu_phase_benchmark": (C.c_int, [P, C.POINTER(Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint64, P]),
         "cr_gpu_render_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning), C.POINTER(EngineStats)]),
         "cr_gpu_autotune_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning)]),
@@ -411,6 +418,16 @@ class GpuScene:
         out = np.zeros((height, width, 3), np.float32)
         check(lib.cr_gpu_film_download(self.handle, out.ctypes.data, out.size))
         return out
+
+    def render_guided(self, camera, options, guide, train_samples=32, probability=0.5, batch=16384, epochs=4,
+                      tuning=None):
+        """cr_gpu_render_guided: returns (film, stats); `guide` is a Guide and keeps its training."""
+        film = np.zeros((options.height, options.width, 3), np.float32)
+        stats = Stats()
+        go = GuideOptions(train_samples, probability, batch, epochs)
+        check(lib.cr_gpu_render_guided(self.handle, C.byref(camera), C.byref(options), guide.handle, C.byref(go),
+                                       film.ctypes.data, C.byref(stats), C.byref(tuning) if tuning else None))
+        return film, stats.as_dict()
 
     def film_encode(self, fmt=ENCODE_SRGB8, exposure=0.0):
         """The last render's film encoded on the device (cr_gpu_film_encode): bytes."""

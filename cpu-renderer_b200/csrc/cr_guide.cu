@@ -401,12 +401,28 @@ void guideInferPaths(cr_guide* gd, cudaStream_t s, const uint32_t* queue, const 
     CR_CUDA(cudaGetLastError());
 }
 
+__global__ void k_guide_weight_sum(const GuideSample* samples, uint64_t n, double* sum) {
+    double a = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        a += samples[i].weight;
+    for (int o = 16; o; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(sum, a);
+}
+
 // Adam steps on device-resident samples: `steps` mini-batches of `batch` consecutive samples
 // (wrapping around), loss weights normalised by the collection's mean weight.
 float guideTrain(cr_guide* gd, cudaStream_t s, const GuideSample* samples, uint64_t n, uint32_t steps, uint32_t batch,
                  float lr, double weightMean) {
     guideAttributes();
     if (n == 0 || steps == 0) return 0.0f;
+    if (weightMean <= 0) {
+        CR_CUDA(cudaMemsetAsync(gd->loss, 0, sizeof(double), s));
+        k_guide_weight_sum<<<256, 256, 0, s>>>(samples, n, gd->loss);
+        double sum = 0;
+        CR_CUDA(cudaMemcpyAsync(&sum, gd->loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        weightMean = sum / static_cast<double>(n);
+    }
     const uint64_t b = std::min<uint64_t>(batch, n);
     const float scale = static_cast<float>(1.0 / (static_cast<double>(b) * (weightMean > 0 ? weightMean : 1.0)));
     double lossHost = 0;

@@ -13,10 +13,11 @@
 #include <cuda_fp16.h>
 
 #include "cr_dev_math.cuh"
+#include "cr_internal.h"
 
 namespace crg {
 
-constexpr int kGuideIn = 64;       // encoded input width (33 features, zero padded)
+constexpr int kGuideIn = 64;       // encoded input width (57 encoded features, zero padded)
 constexpr int kGuideWidth = 64;
 constexpr int kGuideLobes = 8;
 constexpr int kGuideOut = 40;      // 5 per lobe
@@ -28,13 +29,15 @@ constexpr int kGW1 = 0, kGW2 = kGW1 + kGuideWidth * kGuideIn, kGW3 = kGW2 + kGui
 constexpr int kGB1 = kGWCount, kGB2 = kGB1 + kGuideWidth, kGB3 = kGB2 + kGuideWidth, kGB4 = kGB3 + kGuideWidth,
               kGParams = kGB4 + kGuideOutPad;
 constexpr float kLogKappaMin = -3.0f, kLogKappaMax = 9.0f;
+constexpr int kGuideOctaves = 8;
 
-// Inputs: the 9 features, then sin and cos of 2^k * pi * position for k = 0..3.
+// Inputs: the 9 features, then sin and cos of 2^k * pi * position for k = 0..kGuideOctaves-1
+// (57 of the 64 inputs; 8 octaves resolve 1/256 of the scene's extent).
 CR_HD void guideEncode(const float f[kGuideFeatures], float x[kGuideIn]) {
     for (int i = 0; i < kGuideIn; ++i) x[i] = 0.0f;
     for (int i = 0; i < kGuideFeatures; ++i) x[i] = f[i];
     int o = kGuideFeatures;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kGuideOctaves; ++k) {
         const float s = static_cast<float>(1 << k) * kPi;
         for (int d = 0; d < 3; ++d) {
             float sn, cs;
@@ -121,17 +124,53 @@ struct GuideSample {  // one training sample
     float dir[3];
     float weight;   // luminance of the incident radiance along dir / its sampling density
 };
-struct GuidePaths {
-    const float* mixture;   // [path][kGuideOut] network outputs of the path's current vertex
-    float* hitT;            // [path] closest-hit distance (float)
-    GuideRecord* records;   // [path][kGuideRecords]
-    uint32_t* count;        // [path] records in use
-    GuideSample* samples;   // training samples collected
-    unsigned long long* sampleCount;
-    uint64_t sampleCapacity;
-    V3 boundsLo, boundsInv; // position features = (p - lo) * inv
-    float guideProbability; // one-sample MIS: the mixture's share of the directions
-    int record;             // collect training samples
-};
+CR_D GuideRecord* guideRecords(const GuidePathRefs& G, uint32_t path) {
+    return static_cast<GuideRecord*>(G.records) + static_cast<uint64_t>(path) * kGuideRecords;
+}
 
+// Light arriving at a recorded vertex from its own light sample is not light along the
+// recorded direction: it moves the record's base along with the path's radiance.
+CR_D void guideNeeResolved(const GuidePathRefs& G, uint32_t path, V3 added) {
+    const uint32_t n = G.count[path];
+    if (!n) return;
+    GuideRecord& r = guideRecords(G, path)[n - 1];
+    if (!r.neeOpen) return;
+    r.base[0] += added.x; r.base[1] += added.y; r.base[2] += added.z;
+    r.neeOpen = 0;
+}
+
+// A finished path turns its records into training samples: the light that arrived along each
+// recorded direction is (final radiance - base) / throughput after the vertex, and the sample
+// weight is its luminance over the direction's sampling density.
+CR_D void guideFinish(const GuidePathRefs& G, uint32_t path, V3 R) {
+    const uint32_t n = G.count[path];
+    const GuideRecord* rec = guideRecords(G, path);
+    for (uint32_t i = 0; i < n; ++i) {
+        const GuideRecord& r = rec[i];
+        const float lx = r.thr[0] > 0 ? (R.x - r.base[0]) / r.thr[0] : 0.0f;
+        const float ly = r.thr[1] > 0 ? (R.y - r.base[1]) / r.thr[1] : 0.0f;
+        const float lz = r.thr[2] > 0 ? (R.z - r.base[2]) / r.thr[2] : 0.0f;
+        const float w = luminance(V3{fmaxf(lx, 0.0f), fmaxf(ly, 0.0f), fmaxf(lz, 0.0f)}) / r.pdf;
+        if (!(w > 0) || !isfinite(w)) continue;
+        const unsigned long long at = atomicAdd(G.sampleCount, 1ull);
+        if (at >= G.sampleCapacity) continue;
+        GuideSample& out = static_cast<GuideSample*>(G.samples)[at];
+        for (int k = 0; k < kGuideFeatures; ++k) out.feat[k] = r.feat[k];
+        out.dir[0] = r.dir[0]; out.dir[1] = r.dir[1]; out.dir[2] = r.dir[2];
+        out.weight = w;
+    }
+    G.count[path] = 0;
+}
+
+}  // namespace crg
+
+struct cr_guide;
+namespace crg {
+// Host side (cr_guide.cu). Inference for the paths of a shading queue (device count), outputs
+// at out[path * kGuideOut]; Adam steps over device-resident samples (weightMean <= 0: the
+// samples' mean weight, computed on the device). Both run on stream s.
+void guideInferPaths(cr_guide* gd, cudaStream_t s, const uint32_t* queue, const uint32_t* queueCount, uint32_t maxRows,
+                     const PathSoA& st, const float* hitT, const DevScene& S, V3 lo, V3 inv, float* out);
+float guideTrain(cr_guide* gd, cudaStream_t s, const GuideSample* samples, uint64_t n, uint32_t steps, uint32_t batch,
+                 float lr, double weightMean);
 }  // namespace crg

@@ -105,6 +105,20 @@ struct RenderParams {
     DevCamera camera;
 };
 
+// Guided renders only (all null otherwise): the per-path guiding state of cr_guide.cuh.
+struct GuidePathRefs {
+    const float* mixture = nullptr;          // [path][40] network outputs for the path's current vertex
+    float* hitT = nullptr;                   // [path] closest-hit distance
+    void* records = nullptr;                 // GuideRecord [path][kGuideRecords]
+    uint32_t* count = nullptr;               // [path] records in use
+    void* samples = nullptr;                 // GuideSample [sampleCapacity]: training samples collected
+    unsigned long long* sampleCount = nullptr;
+    uint64_t sampleCapacity = 0;
+    float lo[3] = {0, 0, 0}, inv[3] = {0, 0, 0};  // position features = (p - lo) * inv
+    float guideProbability = 0;              // one-sample MIS: share of directions from the network
+    int32_t record = 0;                      // collect training samples
+};
+
 // Path state, structure of arrays over path slots.
 struct PathSoA {
     float4* ray_o;        // origin, tmin
@@ -128,6 +142,7 @@ struct PathSoA {
     float4* sh_c;         // contribution, ignore-triangle bits
     // per-sample radiance of the current chunk, indexed by sample id - chunk start
     float4* out;
+    GuidePathRefs guide;  // zero unless the render is guided
 };
 // bits of PathSoA::flags
 enum : uint32_t { kPathLastDelta = 1u, kPathPrecise = 2u, kPathDead = 4u, kPathShadow = 8u };

@@ -4,6 +4,7 @@
 // both use are templates or static, so each translation unit holds its own instantiation.
 #pragma once
 #include "cr_shade.cuh"
+#include "cr_guide.cuh"
 
 // Minimum resident blocks per SM requested from the register allocator (128-thread blocks).
 // k_trace at 12 (40 registers, some spills to L1) measured ~2 % faster than at 8 or 10 on
@@ -119,6 +120,7 @@ CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     st.pixel[slot] = pixel;
     st.sample[slot] = sample;
     st.depth[slot] = 0;
+    if (st.guide.count) st.guide.count[slot] = 0;
     return true;
 }
 
@@ -138,6 +140,7 @@ CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, 
         R = V3{};
     }
     st.out[O.base + static_cast<uint64_t>(sample) * O.pixels + pixel] = f4(R, 0);
+    if (st.guide.count) guideFinish(st.guide, path, R);
 }
 
 // One iteration of trace()'s bounce loop (render.cpp:240-344) for one path, after its
@@ -145,7 +148,7 @@ CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, 
 // that ends with a queued shadow ray is finished by k_trace next iteration); freed: the path
 // ended and its slot can take a new sample. CLASS specialises the code: kShadeMiss holds only
 // environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeGeneric anything.
-template <int CLASS>
+template <int CLASS, bool GUIDED = false>
 CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
                    const ErrSink& E, unsigned long long* retries, bool& cont, bool& shadow, bool& freed) {
     cont = false; shadow = false; freed = false;
@@ -194,6 +197,19 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
     bool pending = false;
     TRay sh;
     V3 contrib;
+    // Guided renders: at a rough, opaque surface (no delta or transmission lobe) the direction
+    // is drawn from the network's mixture with probability a and from the BSDF otherwise
+    // (one-sample MIS); both MIS weights of trace() then use the combined density.
+    Mixture mix;
+    bool guided = false;
+    float a = 0;
+    if constexpr (GUIDED) {
+        guided = s.transmission <= 0 && s.roughness > 1e-3f;
+        if (guided) {
+            guideDecode(st.guide.mixture + static_cast<uint64_t>(path) * kGuideOut, mix);
+            a = st.guide.guideProbability;
+        }
+    }
     if (CLASS == kShadeNeeNull && P.nee) {
         skipLight(S, rng, P.env_alias != 0);  // zero BSDF: the sample cannot contribute
     } else if (P.nee) {  // render.cpp:262-299
@@ -217,7 +233,11 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
                     sh.d = normalize(delta);
                 }
                 if (ok) {
-                    const float weight = light.delta ? 1 : powerHeuristic(light.pdf, bsdf.pdf);
+                    float dirPdf = bsdf.pdf;
+                    if constexpr (GUIDED) {
+                        if (guided) dirPdf = a * mixturePdf(mix, light.direction) + (1 - a) * bsdf.pdf;
+                    }
+                    const float weight = light.delta ? 1 : powerHeuristic(light.pdf, dirPdf);
                     V3 shadowAbsorption = A;
                     bool shadowInMedium = medium >= 0;
                     if (s.thickness > 0 && dot(wo, s.geometricNormal) * dot(light.direction, s.geometricNormal) < 0) {
@@ -249,7 +269,39 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
             st.flags[path] = flags | kPathDead | kPathShadow;
         }
     };
-    const BsdfSample smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
+    BsdfSample smp;
+    if constexpr (GUIDED) {
+        if (guided) {
+            smp = emptySample();
+            V3 fcos{};
+            float bsdfPdf = 0;
+            if (rng.uniform() < a) {
+                const V3 w = sampleMixture(mix, rng);
+                const BsdfEval e = evaluateBsdf(s, wo, w);
+                if (e.pdf > 0 && maxComponent(e.value) > 0) {
+                    smp.direction = w;
+                    fcos = e.value * fabsf(dot(s.normal, w));
+                    bsdfPdf = e.pdf;
+                }
+            } else {
+                const BsdfSample b = sampleBsdf(s, wo, rng);
+                if (b.ok() && !b.delta) {
+                    smp.direction = b.direction;
+                    fcos = b.weight * b.pdf;
+                    bsdfPdf = b.pdf;
+                }
+            }
+            if (bsdfPdf > 0) {
+                const float pdf = a * mixturePdf(mix, smp.direction) + (1 - a) * bsdfPdf;
+                smp.pdf = pdf;
+                smp.weight = fcos * (1 / pdf);
+            }
+        } else {
+            smp = sampleBsdf(s, wo, rng);
+        }
+    } else {
+        smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
+    }
     if (!smp.ok()) {
         if (pending) queueShadow(true); else finish(R);
         return;
@@ -322,6 +374,26 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
     st.prev_tri[path] = ignore;
     st.depth[path] = depth + 1;
     if (pending) queueShadow(false);
+    if constexpr (GUIDED) {  // remember the vertex: its incident light becomes a training sample
+        if (guided && st.guide.record) {
+            const uint32_t n = st.guide.count[path];
+            if (n < kGuideRecords) {
+                GuideRecord& r = guideRecords(st.guide, path)[n];
+                const float4 ng = S.tri_ng[tri];
+                r.feat[0] = (s.position.x - st.guide.lo[0]) * st.guide.inv[0];
+                r.feat[1] = (s.position.y - st.guide.lo[1]) * st.guide.inv[1];
+                r.feat[2] = (s.position.z - st.guide.lo[2]) * st.guide.inv[2];
+                r.feat[3] = wo.x; r.feat[4] = wo.y; r.feat[5] = wo.z;
+                r.feat[6] = ng.x; r.feat[7] = ng.y; r.feat[8] = ng.z;
+                r.dir[0] = smp.direction.x; r.dir[1] = smp.direction.y; r.dir[2] = smp.direction.z;
+                r.pdf = smp.pdf;
+                r.base[0] = R.x; r.base[1] = R.y; r.base[2] = R.z;
+                r.thr[0] = T.x; r.thr[1] = T.y; r.thr[2] = T.z;
+                r.neeOpen = pending ? 1u : 0u;
+                st.guide.count[path] = n + 1;
+            }
+        }
+    }
     cont = true;
 }
 
@@ -347,6 +419,7 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
     const float4 ra = st.rad[path];
     V3 R = v3(ra);
     if (!blocked) R = R + v3(c);
+    if (st.guide.count) guideNeeResolved(st.guide, path, blocked ? V3{} : v3(c));
     const uint32_t flags = st.flags[path];
     if (flags & kPathDead) { finishPath(P, O, st, path, R, E); return true; }
     st.rad[path] = f4(R, ra.w);
@@ -365,6 +438,7 @@ CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st,
     const bool found = intersect<false, COUNT>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
                                                h, err, &vc);
     st.hit_tri[path] = found ? h.tri : kNoTriangle;
+    if (st.guide.hitT) st.guide.hitT[path] = found ? static_cast<float>(h.t) : 0.0f;
     if (err) raise(E, P, st.pixel[path], st.sample[path], err);
     if (COUNT) {
         atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
@@ -534,7 +608,7 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
     }
 }
 
-template <int CLASS, bool MULTI = false>
+template <int CLASS, bool MULTI = false, bool GUIDED = false>
 __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J) {
     const uint32_t n = q.counts[kCountShade0 + CLASS];
@@ -550,7 +624,7 @@ __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 shadeOne<CLASS>(*pj.S, *pj.P, pj.O, st, path, pj.E, pj.retries, cont, shadow, freed);
                 r = pj.r;
             } else {
-                shadeOne<CLASS>(S, P, outOf(C), st, path, E, &stats[kStatRetries], cont, shadow, freed);
+                shadeOne<CLASS, GUIDED>(S, P, outOf(C), st, path, E, &stats[kStatRetries], cont, shadow, freed);
             }
         }
         warpPush(q.extend[cur ^ 1], &q.counts[kCountExtend0 + (cur ^ 1)], cont, path);

@@ -369,10 +369,20 @@ struct Frames {
     void* user = nullptr;
 };
 
+// A guided render: the network, its online training during the first trainSamples samples per
+// pixel, and the mixture's share of the sampled directions.
+struct GuideRun {
+    cr_guide* gd = nullptr;
+    uint32_t trainSamples = 32;
+    float probability = 0.5f;
+    uint32_t batch = 16384;
+    uint32_t epochs = 4;
+};
+
 // The whole render. filmHost may be NULL (film stays on the device).
 void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, cr_progress_fn progress,
                 void* user, float* filmHost, cr_render_stats* stats, const cr_gpu_tuning& tuning, float* perSample,
-                const Frames& frames = Frames{}) {
+                const Frames& frames = Frames{}, const GuideRun* guide = nullptr) {
     const auto start = std::chrono::steady_clock::now();
     crh::validate_options(o);
     const uint64_t pixels = static_cast<uint64_t>(o.width) * o.height;
@@ -391,7 +401,8 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     // 1M-triangle 1080p workload that measured faster than refilling (regeneration) at every
     // pool/chunk ratio tried (212 vs 200 Msamples/s at its best, 2x pool), and a larger pool
     // amortises the drain tail over more samples (2^22: 177, 2^24: 207, 2^25: 213).
-    uint64_t pool = tuning.paths_per_wave > 0 ? static_cast<uint64_t>(tuning.paths_per_wave) : (uint64_t{1} << 25);
+    uint64_t pool = tuning.paths_per_wave > 0 ? static_cast<uint64_t>(tuning.paths_per_wave)
+                                              : (uint64_t{1} << (guide ? 23 : 25));
     pool = std::max<uint64_t>(1024, std::min<uint64_t>(pool, total));
     const uint64_t chunkBudget = uint64_t{1} << 28;  // 268 M samples = 4 GiB of float4 radiance
     if (tuning.chunk_log2 && (tuning.chunk_log2 < 16 || tuning.chunk_log2 > 28))
@@ -421,6 +432,40 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     W.ensureOut(static_cast<size_t>(chunk));
     g.ensureFilm(pixels);
     if (perSample) W.ensurePacked(static_cast<size_t>(chunk));
+    // Guided renders: per-path network outputs and hit distances for the pool, records and the
+    // training-sample store for the training chunks (one sample per pixel each).
+    DevAlloc guideMem;
+    struct ReleaseAtEnd {
+        DevAlloc& m;
+        cudaStream_t s;
+        ~ReleaseAtEnd() { cudaStreamSynchronize(s); m.release(); }
+    } releaseGuide{guideMem, g.stream};
+    PathSoA st = W.st;  // after the workspace buffers above exist
+    const uint64_t trainTotal = guide ? std::min<uint64_t>(total, static_cast<uint64_t>(guide->trainSamples) * pixels) : 0;
+    float* guideOut = nullptr;
+    GuideSample* guideSamples = nullptr;
+    uint64_t guideCapacity = 0;
+    if (guide) {
+        guideOut = guideMem.alloc<float>(pool * kGuideOut);
+        st.guide.mixture = guideOut;
+        st.guide.hitT = guideMem.alloc<float>(pool);
+        const uint64_t trainPool = std::min<uint64_t>(pool, pixels);
+        st.guide.records = guideMem.alloc<GuideRecord>(trainPool * kGuideRecords);
+        st.guide.count = guideMem.alloc<uint32_t>(trainPool);
+        guideCapacity = std::min<uint64_t>(uint64_t{1} << 22, pixels * kGuideRecords);
+        guideSamples = guideMem.alloc<GuideSample>(guideCapacity);
+        st.guide.samples = guideSamples;
+        st.guide.sampleCount = guideMem.alloc<unsigned long long>(1);
+        st.guide.sampleCapacity = guideCapacity;
+        for (int k = 0; k < 3; ++k) {
+            const float lo = g.dev.root_lo[k], ext = g.dev.root_hi[k] - lo;
+            st.guide.lo[k] = lo;
+            st.guide.inv[k] = ext > 0 ? 1.0f / ext : 0.0f;
+        }
+        st.guide.guideProbability = guide->probability;
+        st.guide.record = 1;
+        CR_CUDA(cudaMemsetAsync(st.guide.sampleCount, 0, sizeof(unsigned long long), g.stream));
+    }
     if (!W.hostCounts) CR_CUDA(cudaMallocHost(&W.hostCounts, kCountWords * sizeof(uint32_t)));
     if (!W.hostStats) CR_CUDA(cudaMallocHost(&W.hostStats, kStatWords * sizeof(unsigned long long)));
     cudaStream_t s = g.stream;
@@ -454,16 +499,27 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     auto lastProgress = start;
     bool errored = false;
     const int batch = 8;
-    for (uint64_t c0 = 0; c0 < total && !errored; c0 += chunk) {
-        const Chunk C{c0, std::min<uint64_t>(total, c0 + chunk), pixels};
+    uint64_t step = chunk;
+    for (uint64_t c0 = 0; c0 < total && !errored; c0 += step) {
+        // guided renders train between one-sample-per-pixel chunks, then render in full chunks
+        const bool training = guide && c0 < trainTotal;
+        step = training ? std::min<uint64_t>(pixels, trainTotal - c0) : chunk;
+        if (guide && !training && st.guide.count) {  // training is over: stop recording
+            st.guide.count = nullptr;
+            st.guide.records = nullptr;
+            st.guide.record = 0;
+        }
+        const Chunk C{c0, std::min<uint64_t>(total, c0 + step), pixels};
         ++chunks;
         // the chunk's ids are issued from c0
         CR_CUDA(cudaMemsetAsync(W.counts, 0, kCountWords * sizeof(uint32_t), s));
         const unsigned long long issuedStart = c0;
         CR_CUDA(cudaMemcpyAsync(W.stats + kStatIssued, &issuedStart, sizeof(issuedStart), cudaMemcpyHostToDevice, s));
-        k_pool_init<<<W.gridSmall, 128, 0, s>>>(W.q, static_cast<uint32_t>(pool));
+        // a training chunk uses only as many slots as it has samples: its paths' records cover them
+        const uint64_t chunkPool = training ? std::min<uint64_t>(pool, step) : pool;
+        k_pool_init<<<W.gridSmall, 128, 0, s>>>(W.q, static_cast<uint32_t>(chunkPool));
         ++launches;
-        const uint64_t maxIterations = ((C.c1 - C.c0) / pool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
+        const uint64_t maxIterations = ((C.c1 - C.c0) / chunkPool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
         uint64_t iter = 0;
         int cur = 0;
         std::vector<std::pair<size_t, int>> timed;
@@ -478,14 +534,24 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     if (timePhases) { CR_CUDA(cudaEventRecord(W.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
                     ++launches;
                 };
-                rec(2, [&] { k_regen<false><<<W.gridRegen, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
+                rec(2, [&] { k_regen<false><<<W.gridRegen, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
                 rec(0, [&] {
-                    if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{});
-                    else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{});
+                    if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                 });
-                rec(1, [&] { k_shade<kShadeMiss><<<W.gridShadeMiss, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}); });
-                rec(1, [&] { k_shade<kShadeNeeNull><<<W.gridShadeLight, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}); });
-                rec(1, [&] { k_shade<kShadeGeneric><<<W.gridShade, 128, 0, s>>>(g.dev, P, W.st, W.q, cur, C, E, W.stats, JobTable{}); });
+                rec(1, [&] { k_shade<kShadeMiss><<<W.gridShadeMiss, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                rec(1, [&] { k_shade<kShadeNeeNull><<<W.gridShadeLight, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                if (guide) {
+                    rec(1, [&] {
+                        guideInferPaths(guide->gd, s, W.q.shade[kShadeGeneric], W.q.counts + kCountShade0 + kShadeGeneric,
+                                        static_cast<uint32_t>(pool), st, st.guide.hitT, g.dev,
+                                        V3{st.guide.lo[0], st.guide.lo[1], st.guide.lo[2]},
+                                        V3{st.guide.inv[0], st.guide.inv[1], st.guide.inv[2]}, guideOut);
+                    });
+                    rec(1, [&] { k_shade<kShadeGeneric, false, true><<<W.gridShade, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                } else {
+                    rec(1, [&] { k_shade<kShadeGeneric><<<W.gridShade, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                }
                 cur ^= 1;
                 ++iter;
                 ++iterations;
@@ -516,8 +582,20 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
             }
         }
         if (errored) break;
-        k_accumulate<<<W.gridSmall, 128, 0, s>>>(W.st.out, C, g.acc);
+        k_accumulate<<<W.gridSmall, 128, 0, s>>>(st.out, C, g.acc);
         ++launches;
+        if (training) {  // Adam over this chunk's samples; the next chunk uses the new weights
+            unsigned long long collected = 0;
+            CR_CUDA(cudaMemcpyAsync(&collected, st.guide.sampleCount, sizeof(collected), cudaMemcpyDeviceToHost, s));
+            CR_CUDA(cudaStreamSynchronize(s));
+            const uint64_t n = std::min<uint64_t>(collected, guideCapacity);
+            if (n) {
+                const uint32_t steps = static_cast<uint32_t>(guide->epochs * ((n + guide->batch - 1) / guide->batch));
+                guideTrain(guide->gd, s, guideSamples, n, steps, guide->batch, 1e-3f, -1.0);
+                launches += 2ull * steps + 1;
+            }
+            CR_CUDA(cudaMemsetAsync(st.guide.sampleCount, 0, sizeof(unsigned long long), s));
+        }
         if (frames.every) {
             const uint32_t done = static_cast<uint32_t>(C.c1 / pixels);
             k_film<<<W.gridSmall, 128, 0, s>>>(g.acc, g.film, pixels, done);
@@ -529,7 +607,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         }
         if (perSample) {
             const uint64_t n = C.c1 - C.c0;
-            k_pack_samples<<<W.gridSmall, 128, 0, s>>>(W.st.out, n, W.packed);
+            k_pack_samples<<<W.gridSmall, 128, 0, s>>>(st.out, n, W.packed);
             CR_CUDA(cudaMemcpyAsync(perSample + 3 * C.c0, W.packed, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
             CR_CUDA(cudaStreamSynchronize(s));
         }
@@ -909,6 +987,24 @@ cr_status cr_gpu_render_progressive(cr_gpu_scene* g, const cr_camera* camera, co
         Frames f;
         f.every = every_samples; f.format = format; f.exposure = exposure; f.fn = on_frame; f.user = user;
         renderImpl(*g, *camera, *options, nullptr, nullptr, film_rgb, stats, defaults(tuning), nullptr, f);
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_render_guided(cr_gpu_scene* g, const cr_camera* camera, const cr_render_options* options, cr_guide* guide,
+                               const cr_guide_options* gopt, float* film_rgb, cr_render_stats* stats, const cr_gpu_tuning* tuning) {
+    try {
+        if (!g || !camera || !options || !guide) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        GuideRun run;
+        run.gd = guide;
+        if (gopt) {
+            run.trainSamples = gopt->train_samples;
+            if (gopt->guide_probability > 0) run.probability = std::min(gopt->guide_probability, 0.95f);
+            if (gopt->batch) run.batch = gopt->batch;
+            if (gopt->epochs) run.epochs = gopt->epochs;
+        }
+        renderImpl(*g, *camera, *options, nullptr, nullptr, film_rgb, stats, defaults(tuning), nullptr, Frames{}, &run);
         return CR_OK;
     } catch (const std::exception& e) { return fail(e); }
 }

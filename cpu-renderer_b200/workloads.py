@@ -158,11 +158,12 @@ def _sphere_mesh(slices=77, stacks=18):
 
 
 def sky_image(width=2048, height=1024, seed=GRID_SEED + 1, sun_elevation_deg=35.0, sun_azimuth_deg=60.0,
-              sun_diameter_deg=0.5, sun_radiance=5e4):
-    """RGBA float32 (H, W, 4): log-normal(0, 1) grey texels and a sun disk."""
+              sun_diameter_deg=0.5, sun_radiance=5e4, background=True):
+    """RGBA float32 (H, W, 4): log-normal(0, 1) grey texels (black without background) and a
+    sun disk."""
     rng = np.random.default_rng(seed)
     img = np.ones((height, width, 4), np.float32)
-    img[..., :3] = np.exp(rng.normal(0.0, 1.0, size=(height, width, 1))).astype(np.float32)
+    img[..., :3] = np.exp(rng.normal(0.0, 1.0, size=(height, width, 1))).astype(np.float32) if background else 0.0
     theta = (np.arange(height) + 0.5) / height * math.pi
     phi = ((np.arange(width) + 0.5) / width - 0.5) * 2 * math.pi
     st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
@@ -243,6 +244,49 @@ def sphere_grid_scene(seed=GRID_SEED, width=1920, height=1080, samples=64, bounc
     return dict(triangles=triangles, materials=mats, lights=None, camera=camera, options=options,
                 env_image=sky_image() if sky else None,
                 name="sphere-grid-1M-1920x1080-64spp-d16")
+
+
+def caustic_scene(width=320, height=180, samples=64, bounces=16):
+    """The learned-proposal workload: the sphere grid with every sphere a smooth closed
+    dielectric of IOR 1.5 or a GGX conductor of roughness 0.05 (the same 50/50 draw), lit only
+    by the sun disk (black sky). The ground keeps its rough, non-metallic material: it is the
+    surface that receives the caustics (with every surface specular or near-specular, no light
+    path through the dielectrics could end at a surface the camera sees diffusely)."""
+    sc = sphere_grid_scene(width=width, height=height, samples=samples, bounces=bounces, sky=False)
+    m = sc["materials"]
+    spheres = len(m) - 1
+    metal = m["metallic"][:spheres] == 1.0
+    m["roughness"][:spheres][metal] = 0.05
+    m["ior"][:spheres][~metal] = 1.5
+    sc["env_image"] = sky_image(width=1024, height=512, background=False)
+    sc["name"] = f"caustic-sphere-grid-{width}x{height}"
+    return sc
+
+
+def sunlit_room_scene(width=64, height=64, samples=64, bounces=8, hole=0.2):
+    """A closed diffuse 2x2x2 room lit only by the sun disk through a square opening in the
+    ceiling (half-width `hole`): the sun lands on a patch of the back wall and everything else
+    is lit by that patch, the case where BSDF sampling rarely finds the light and a guide can."""
+    mats = new_materials(2)
+    for m, col in ((mats[0], 0.75), (mats[1], 0.6)):
+        m["metallic"] = 0.0
+        m["roughness"] = 1.0
+        m["base_color"][:3] = col
+    tris = []
+    lo, hi = -1.0, 1.0
+    _quad(tris, (lo, 0, lo), (hi, 0, lo), (hi, 0, hi), (lo, 0, hi), 1, inward=(0, 1, 0))      # floor
+    _quad(tris, (lo, 0, lo), (lo, 2, lo), (lo, 2, hi), (lo, 0, hi), 0, inward=(1, 0, 0))      # left
+    _quad(tris, (hi, 0, lo), (hi, 2, lo), (hi, 2, hi), (hi, 0, hi), 0, inward=(-1, 0, 0))     # right
+    _quad(tris, (lo, 0, lo), (hi, 0, lo), (hi, 2, lo), (lo, 2, lo), 0, inward=(0, 0, 1))      # back
+    _quad(tris, (lo, 0, hi), (hi, 0, hi), (hi, 2, hi), (lo, 2, hi), 0, inward=(0, 0, -1))     # front
+    h = hole  # ceiling around the opening [-h, h]^2
+    for (x0, x1, z0, z1) in ((lo, hi, lo, -h), (lo, hi, h, hi), (lo, -h, -h, h), (h, hi, -h, h)):
+        _quad(tris, (x0, 2, z0), (x1, 2, z0), (x1, 2, z1), (x0, 2, z1), 0, inward=(0, -1, 0))
+    camera = Camera.make(position=(0, 1, 0.98), forward=(0, 0, -1), right=(1, 0, 0), up=(0, 1, 0),
+                         yfov=math.radians(70.0))
+    options = Options.make(width=width, height=height, samples=samples, bounces=bounces, threads=0, seed=42)
+    return dict(triangles=np.array(tris, dtype=tris[0].dtype), materials=mats, camera=camera, options=options,
+                env_image=sky_image(width=1024, height=512, background=False), name="sunlit-room")
 
 
 MIX_SEED = 0x5EED0003

@@ -392,7 +392,7 @@ cr_status cr_gpu_phase_benchmark(cr_gpu_scene* scene, const cr_camera* camera, i
 /* ---- learned path guiding -----------------------------------------------------------------------
  * No counterpart in the reference. A cr_guide is a small network on one device: 4 dense layers
  * 64 wide map a shading point (position scaled to the scene bounds, outgoing direction,
- * geometric normal; 9 features, encoded to 64 inputs) to a mixture of 8 von Mises-Fisher
+ * geometric normal; 9 features plus sin/cos of 8 octaves of the position, 64 inputs) to a mixture of 8 von Mises-Fisher
  * lobes (40 outputs: per lobe the mixture logit, log kappa and the unnormalised mean). Its
  * weights are FP32 masters (trained by Adam) with an FP16 copy used by inference on the tensor
  * cores (FP32 accumulation). cr_gpu_render_guided trains it online on the tracer's own radiance
@@ -413,6 +413,23 @@ cr_status cr_guide_gradients(cr_guide* guide, const float* samples, uint64_t n, 
  * normalised by their mean; *loss receives the last batch's loss. */
 cr_status cr_guide_train(cr_guide* guide, const float* samples, uint64_t n, uint32_t steps, uint32_t batch, float lr,
                          float* loss);
+
+/* Guided render: cr::render's estimator with the directions at rough, opaque surfaces drawn by
+ * one-sample MIS from the guide's mixture (probability guide_probability) and the BSDF, the
+ * combined density used in both MIS weights of trace(), so the film stays unbiased. During the
+ * first train_samples samples per pixel the render runs one sample per pixel at a time and,
+ * after each, trains the guide (Adam, lr 1e-3, `epochs` passes in mini-batches of `batch`) on
+ * the light that arrived along each guided direction. The guide keeps its trained weights.
+ * gopt may be NULL: train 32 samples, probability 0.5, batch 16384, 4 epochs. */
+typedef struct cr_guide_options {
+    uint32_t train_samples;
+    float guide_probability;
+    uint32_t batch;
+    uint32_t epochs;
+} cr_guide_options;
+cr_status cr_gpu_render_guided(cr_gpu_scene* scene, const cr_camera* camera, const cr_render_options* options,
+                               cr_guide* guide, const cr_guide_options* gopt, float* film_rgb,
+                               cr_render_stats* stats, const cr_gpu_tuning* tuning);
 
 /* ---- many renders in one path pool ------------------------------------------------------------
  * No counterpart in the reference, which renders one image per cr::render call. The engine

@@ -26,13 +26,17 @@ def fp16_round(p):
     return np.asarray(p, np.float32).astype(np.float16).astype(np.float64)
 
 
+OCTAVES = 8
+
+
 def encode(features):
-    """features (n, 9) -> inputs (n, 64): the features, then sin and cos of 2^k pi position."""
+    """features (n, 9) -> inputs (n, 64): the features, then sin and cos of 2^k pi position,
+    k = 0..7 (57 inputs, the rest zero)."""
     f = np.asarray(features, np.float64)
     x = np.zeros((len(f), IN))
     x[:, :FEATURES] = f
     o = FEATURES
-    for k in range(4):
+    for k in range(OCTAVES):
         s = float(1 << k) * math.pi
         for d in range(3):
             x[:, o] = np.sin(s * f[:, d])

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <exception>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -23,15 +24,72 @@ struct CudaError : crh::Error {
 #define CR_CUDA(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) throw crd::CudaError(e_, #call); } while (0)
 
 // Device allocation owned by a scene.
+// Device blocks given back by DevAlloc::release are kept per device for reuse, up to
+// kBlockCacheBytes: handing large blocks back to the driver (cudaFree) occasionally stalls for
+// hundreds of milliseconds, and a scene created again with the same array sizes then reuses its
+// blocks at once. A block is reused for requests of at least half its size. An allocation that
+// fails empties the device's cache and tries again.
+class BlockCache {
+  public:
+    static constexpr size_t kBlockCacheBytes = size_t{48} << 30;
+    static BlockCache& get() {
+        static BlockCache* c = new BlockCache();  // lives until the process exits
+        return *c;
+    }
+    // A cached block of at least `bytes` (and at most twice that), with its own size; or null.
+    std::pair<void*, size_t> take(int device, size_t bytes) {
+        std::lock_guard<std::mutex> lock(m_);
+        auto& bin = blocks_[device];
+        auto it = bin.lower_bound(bytes);
+        if (it == bin.end() || it->first > 2 * bytes) return {nullptr, 0};
+        const std::pair<void*, size_t> b{it->second, it->first};
+        held_[device] -= it->first;
+        bin.erase(it);
+        return b;
+    }
+    void give(int device, void* p, size_t bytes) {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            if (held_[device] + bytes <= kBlockCacheBytes) {
+                blocks_[device].emplace(bytes, p);
+                held_[device] += bytes;
+                return;
+            }
+        }
+        cudaFree(p);
+    }
+    void flush(int device) {
+        std::lock_guard<std::mutex> lock(m_);
+        for (auto& b : blocks_[device]) cudaFree(b.second);
+        blocks_[device].clear();
+        held_[device] = 0;
+    }
+
+  private:
+    std::mutex m_;
+    std::map<int, std::multimap<size_t, void*>> blocks_;
+    std::map<int, size_t> held_;
+};
+
 struct DevAlloc {
-    std::vector<void*> blocks;
+    std::vector<std::pair<void*, size_t>> blocks;
     uint64_t bytes = 0;
     template <class T> T* alloc(size_t count) {
         if (count == 0) count = 1;
-        void* p = nullptr;
-        CR_CUDA(cudaMalloc(&p, count * sizeof(T)));
-        blocks.push_back(p);
-        bytes += count * sizeof(T);
+        const size_t want = count * sizeof(T);
+        int device = 0;
+        CR_CUDA(cudaGetDevice(&device));
+        auto [p, have] = BlockCache::get().take(device, want);
+        if (!p) {
+            if (cudaMalloc(&p, want) != cudaSuccess) {
+                cudaGetLastError();
+                BlockCache::get().flush(device);
+                CR_CUDA(cudaMalloc(&p, want));
+            }
+            have = want;
+        }
+        blocks.push_back({p, have});
+        bytes += want;
         return static_cast<T*>(p);
     }
     template <class T> T* upload(const T* src, size_t count, cudaStream_t s) {
@@ -39,8 +97,11 @@ struct DevAlloc {
         if (count) CR_CUDA(cudaMemcpyAsync(d, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
         return d;
     }
+    // The caller has finished every use of the blocks (its streams are synchronised).
     void release() {
-        for (void* p : blocks) cudaFree(p);
+        int device = 0;
+        cudaGetDevice(&device);
+        for (auto& b : blocks) BlockCache::get().give(device, b.first, b.second);
         blocks.clear();
         bytes = 0;
     }

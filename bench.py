@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--rate", type=float, default=40.0, help="serve: arrivals per second")
     ap.add_argument("--literal-clutter", action="store_true",
                     help="batch/serve: keep config 1's triangle sizes at every triangle count")
+    ap.add_argument("--engine-iters", type=int, default=0,
+                    help="serve: iterations between the engine's host checks (0: the engine's default)")
     ap.add_argument("--mix-scale", type=float, default=1.0,
                     help="batch/serve: scale every job's width and height (quick runs)")
     return ap.parse_args()
@@ -415,7 +417,8 @@ def run_serve(args):
 
     samples = sum(w * h * spp for _, _, (w, h), spp in stream)
     # warm-up: a few requests through a server, then the measured stream
-    srv = crgpu.Server(0)
+    tuning = crgpu.EngineTuning.make(iterations_per_step=args.engine_iters) if args.engine_iters else None
+    srv = crgpu.Server(0, tuning)
     warm = [spec(r) for r in stream[: max(1, args.warmup)]]
     for t in [srv.submit(j) for j in warm]:
         srv.wait(t)
@@ -439,7 +442,7 @@ def run_serve(args):
     served = samples / (fin.max() - sub.min()) / 1e6
     # the same requests as one batch
     t0 = time.perf_counter()
-    crgpu.render_batch([spec(r) for r in stream])
+    crgpu.render_batch([spec(r) for r in stream], tuning)
     batched = samples / (time.perf_counter() - t0) / 1e6
     pct = lambda a, q: float(np.percentile(a, q)) * 1e3
     line = {
@@ -449,7 +452,7 @@ def run_serve(args):
         "config": {"workload": "serve-poisson", "requests": len(stream), "rate_per_s": args.rate, "scenes": len(scenes),
                    "env": "1024x512 per scene", "frames": "sRGB8 every 4 spp", "samples": int(samples),
                    "clutter": "literal config-1 sizes" if args.literal_clutter else "area-preserving sizes",
-                   "mix_scale": args.mix_scale},
+                   "mix_scale": args.mix_scale, "iterations_per_step": args.engine_iters or 8},
         "time_to_first_4spp_ms": {"p50": pct(ttff, 50), "p99": pct(ttff, 99)},
         "time_to_completion_ms": {"p50": pct(ttc, 50), "p99": pct(ttc, 99)},
         "throughput": {"served": served, "batched": batched, "unit": "Msamples/s", "served_over_batched": served / batched},

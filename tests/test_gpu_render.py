@@ -128,6 +128,25 @@ def test_determinism_across_wave_sizes(crgpu, gpu):
     assert a.tobytes() == b.tobytes() == c.tobytes() == d.tobytes()
 
 
+@pytest.mark.parametrize("scene", ["room", "sphere_grid"])
+def test_traversals_render_the_same_film(crgpu, gpu, scene):
+    """The FP32-box traversal and the FP64 exact traversal find the same hits, so the films
+    are identical bit for bit."""
+    if scene == "room":
+        sc = workloads.room_scene()
+        g = gpu_scene(crgpu, sc)
+    else:
+        sc = workloads.sphere_grid_scene(width=160, height=90, samples=4, bounces=8)
+        g = gpu_scene(crgpu, sc, env=crgpu.env_desc(image=sc["env_image"]))
+    cam, opt = sc["camera"], sc["options"]
+    films = []
+    for exact in (0, 1):
+        t = Tuning()
+        t.exact_traversal = exact
+        films.append(g.render(cam, opt, tuning=t)[0].tobytes())
+    assert films[0] == films[1]
+
+
 def test_film_is_the_ordered_double_sum_of_samples(crgpu, gpu):
     sc = workloads.room_scene()
     g = gpu_scene(crgpu, sc)

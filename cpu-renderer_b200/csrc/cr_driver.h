@@ -71,6 +71,54 @@ class BlockCache {
     std::map<int, size_t> held_;
 };
 
+// Page-locked host blocks kept for reuse by scene uploads: copies from page-locked memory run
+// asynchronously at the link's full rate, and pinning fresh memory for every upload would cost
+// more than the copy itself. At most kHeld bytes stay cached; blocks live until process exit.
+class PinnedCache {
+  public:
+    static PinnedCache& get() {
+        static PinnedCache* c = new PinnedCache;  // never destroyed: outlives the CUDA runtime's users
+        return *c;
+    }
+    // A block of at least `bytes` (the cached block's own size is returned), or {nullptr, 0}
+    // when page-locked memory cannot be had.
+    std::pair<void*, size_t> take(size_t bytes) {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            auto it = free_.lower_bound(bytes);
+            if (it != free_.end()) {
+                const std::pair<void*, size_t> r{it->second, it->first};
+                held_ -= it->first;
+                free_.erase(it);
+                return r;
+            }
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return {nullptr, 0};
+        }
+        return {p, bytes};
+    }
+    void give(void* p, size_t bytes) {
+        std::lock_guard<std::mutex> lock(m_);
+        free_.insert({bytes, p});
+        held_ += bytes;
+        while (held_ > kHeld && !free_.empty()) {
+            auto it = free_.begin();
+            cudaFreeHost(it->second);
+            held_ -= it->first;
+            free_.erase(it);
+        }
+    }
+
+  private:
+    static constexpr size_t kHeld = size_t{1} << 31;
+    std::mutex m_;
+    std::multimap<size_t, void*> free_;
+    size_t held_ = 0;
+};
+
 struct DevAlloc {
     std::vector<std::pair<void*, size_t>> blocks;
     uint64_t bytes = 0;

@@ -488,8 +488,29 @@ void build_lights(const cr_triangle* triangles, uint64_t count, const cr_materia
                   const cr_punctual_light* lights, uint32_t lightCount, double envIntegral, LightTables& out) {
     out = LightTables{};
     out.triangleProbability.assign(count, 0.0f);
+    // The scene box and the emitters' weights in parallel: positions are finite after
+    // finalize, so min/max in any order give the same box; the weights go into per-part lists
+    // that are then read in triangle order, so the running total below is summed in the
+    // reference's order.
+    constexpr uint64_t kParts = 64;
+    std::vector<Bounds> partBox(kParts);
+    std::vector<std::vector<std::pair<uint32_t, double>>> partEmitters(kParts);
+    parallel_for(kParts, [&](uint64_t pb, uint64_t pe) {
+        for (uint64_t part = pb; part < pe; ++part) {
+            const uint64_t b = count * part / kParts, e = count * (part + 1) / kParts;
+            Bounds local;
+            for (uint64_t i = b; i < e; ++i) {
+                const cr_triangle& t = triangles[i];
+                local.expand(triangleBounds(t));
+                const cr_material& m = materials[t.material];
+                const double w = static_cast<double>(t.area) * pi * luminance(v3(m.emission)) * (m.double_sided ? 2 : 1);
+                if (w > 0) partEmitters[part].push_back({static_cast<uint32_t>(i), w});
+            }
+            partBox[part] = local;
+        }
+    }, 1);
     Bounds box;
-    for (uint64_t i = 0; i < count; ++i) box.expand(triangleBounds(triangles[i]));
+    for (const Bounds& b : partBox) box.expand(b);
     const double radius2 = count == 0 ? 1 : std::max(1.0, static_cast<double>(lengthSquared(box.hi - box.lo)) * 0.25);
     double total = 0;
     auto add = [&](uint32_t type, uint32_t index, double weight) {
@@ -500,12 +521,8 @@ void build_lights(const cr_triangle* triangles, uint64_t count, const cr_materia
         add(crg::kLightPunctual, i, static_cast<double>(luminance(v3(l.color))) * l.intensity *
                                         (l.type == CR_LIGHT_DIRECTIONAL ? pi * radius2 : 4 * pi));
     }
-    for (uint64_t i = 0; i < count; ++i) {
-        const cr_triangle& t = triangles[i];
-        const cr_material& m = materials[t.material];
-        add(crg::kLightTriangle, static_cast<uint32_t>(i),
-            static_cast<double>(t.area) * pi * luminance(v3(m.emission)) * (m.double_sided ? 2 : 1));
-    }
+    for (const auto& part : partEmitters)
+        for (const auto& [index, weight] : part) add(crg::kLightTriangle, index, weight);
     add(crg::kLightEnvironment, 0, envIntegral * pi * radius2);
     double last = 0, cumulative = 0;
     for (auto& e : out.entries) {

@@ -25,9 +25,11 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <new>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -140,6 +142,92 @@ Workspace& workspaceFor(int device) {
 
 namespace {
 
+template <class T> struct ArrayView {
+    const T* p;
+    size_t n;
+    size_t size() const { return n; }
+    bool empty() const { return n == 0; }
+    const T& operator[](size_t i) const { return p[i]; }
+};
+
+// One host block for the arrays a scene upload builds (page-locked when that can be had, so
+// their copies run asynchronously). The destructor waits for the stream's copies before the
+// block goes back to the cache.
+class Staging {
+  public:
+    Staging(cudaStream_t s, size_t bytes) : s_(s) {
+        auto [q, have] = PinnedCache::get().take(bytes);
+        if (q) { p_ = static_cast<unsigned char*>(q); size_ = have; pinned_ = true; }
+        else { fallback_.reset(new unsigned char[bytes]); p_ = fallback_.get(); size_ = bytes; }
+    }
+    Staging(const Staging&) = delete;
+    Staging& operator=(const Staging&) = delete;
+    ~Staging() {
+        cudaStreamSynchronize(s_);
+        if (pinned_) PinnedCache::get().give(p_, size_);
+    }
+    static size_t bytesFor(size_t bytes) { return (bytes + 255) / 256 * 256; }
+    template <class T> T* carve(size_t count) {
+        T* r = reinterpret_cast<T*>(p_ + used_);
+        used_ += bytesFor(count * sizeof(T));
+        if (used_ > size_) throw std::logic_error("staging block too small");
+        return r;
+    }
+
+  private:
+    cudaStream_t s_;
+    unsigned char* p_ = nullptr;
+    size_t size_ = 0, used_ = 0;
+    bool pinned_ = false;
+    std::unique_ptr<unsigned char[]> fallback_;
+};
+
+// Parts of a scene upload that run on host threads beside the caller's: task k runs on its
+// own thread with the scene's device current and copies on stream(k); join(k) waits for the
+// task and its copies and rethrows its exception. The destructor joins whatever is left.
+class SideWork {
+  public:
+    static constexpr int kTasks = 2;
+    explicit SideWork(int device) : device_(device) {
+        for (int k = 0; k < kTasks; ++k) {
+            const cudaError_t e = cudaStreamCreateWithFlags(&streams_[k], cudaStreamNonBlocking);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                for (int j = 0; j < k; ++j) cudaStreamDestroy(streams_[j]);
+                throw CudaError(e, "cudaStreamCreateWithFlags");
+            }
+        }
+    }
+    SideWork(const SideWork&) = delete;
+    SideWork& operator=(const SideWork&) = delete;
+    cudaStream_t stream(int k) const { return streams_[k]; }
+    void run(int k, std::function<void()> fn) {
+        threads_[k] = std::thread([this, k, fn = std::move(fn)] {
+            try {
+                CR_CUDA(cudaSetDevice(device_));
+                fn();
+                CR_CUDA(cudaStreamSynchronize(streams_[k]));
+            } catch (...) {
+                errors_[k] = std::current_exception();
+            }
+        });
+    }
+    void join(int k) {
+        if (threads_[k].joinable()) threads_[k].join();
+        if (errors_[k]) std::rethrow_exception(errors_[k]);
+    }
+    ~SideWork() {
+        for (auto& t : threads_) if (t.joinable()) t.join();
+        for (auto st : streams_) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
+    }
+
+  private:
+    int device_;
+    cudaStream_t streams_[kTasks] = {};
+    std::thread threads_[kTasks];
+    std::exception_ptr errors_[kTasks];
+};
+
 // Build the device scene: geometry in leaf order, node pairs, materials, lights, environment.
 void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_desc& env) {
     const uint64_t n = d.triangle_count;
@@ -168,15 +256,52 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
             if (im.width <= 0 || im.height <= 0 || !im.pixels) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "Texture image dimensions do not match its pixels");
         }
     }
-    // BVH: the caller's (the reference's own node array) or ours.
-    std::vector<cr_bvh_node> nodes;
-    std::vector<uint32_t> indices;
-    if (d.bvh_nodes && d.bvh_node_count) {
-        nodes.assign(d.bvh_nodes, d.bvh_nodes + d.bvh_node_count);
-        indices.assign(d.bvh_indices, d.bvh_indices + d.bvh_index_count);
-    } else {
-        crh::build_bvh(d.triangles, n, nodes, indices);
-    }
+    // The triangle records go to the device unchanged: that copy (the largest, from the caller's
+    // memory) starts on a helper thread, and the environment tables are built and copied on
+    // another, while this thread prepares the geometry. Errors keep their order: the helpers
+    // are joined where their step stood in the sequential upload.
+    cudaStream_t s = g.stream;
+    DevScene& S = g.dev;
+    S = DevScene{};
+    crh::EnvTables& E = g.env;
+    DevAlloc envMem;  // the environment thread's blocks, handed to the scene when it is done
+    struct AdoptBlocks {
+        DevAlloc& from;
+        DevAlloc& to;
+        ~AdoptBlocks() {
+            to.blocks.insert(to.blocks.end(), from.blocks.begin(), from.blocks.end());
+            to.bytes += from.bytes;
+            from.blocks.clear();
+            from.bytes = 0;
+        }
+    } adopt{envMem, g.geometry};
+    SideWork side(g.device);
+    S.tris = g.geometry.alloc<cr_triangle>(n);
+    side.run(0, [&, dst = const_cast<cr_triangle*>(S.tris)] {
+        if (n) CR_CUDA(cudaMemcpyAsync(dst, d.triangles, n * sizeof(cr_triangle), cudaMemcpyHostToDevice, side.stream(0)));
+    });
+    side.run(1, [&] {
+        crh::build_environment(env, E);
+        if (E.hasImage) {
+            const cudaStream_t es = side.stream(1);
+            const size_t px = static_cast<size_t>(E.width) * E.height;
+            S.env_pixels = envMem.upload(reinterpret_cast<const float4*>(env.pixels), px, es);
+            S.env_cdf = envMem.upload(E.cdf.data(), E.cdf.size(), es);
+            S.env_pdf = envMem.upload(E.pdf.data(), E.pdf.size(), es);
+            S.env_row_cos = envMem.upload(E.rowCos.data(), E.rowCos.size(), es);
+            S.env_coarse = envMem.upload(E.coarse.data(), E.coarse.size(), es);
+        }
+    });
+    // BVH: the caller's (the reference's own node array, read in place) or ours.
+    std::vector<cr_bvh_node> ownNodes;
+    std::vector<uint32_t> ownIndices;
+    if (d.bvh_index_count && !d.bvh_indices) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "bvh_indices is NULL");
+    const bool callerBvh = d.bvh_nodes && d.bvh_node_count;
+    if (!callerBvh) crh::build_bvh(d.triangles, n, ownNodes, ownIndices);
+    const ArrayView<cr_bvh_node> nodes = callerBvh ? ArrayView<cr_bvh_node>{d.bvh_nodes, d.bvh_node_count}
+                                                   : ArrayView<cr_bvh_node>{ownNodes.data(), ownNodes.size()};
+    const ArrayView<uint32_t> indices = callerBvh ? ArrayView<uint32_t>{d.bvh_indices, d.bvh_index_count}
+                                                  : ArrayView<uint32_t>{ownIndices.data(), ownIndices.size()};
     // Structure checks: adjacent children at odd indices, leaf ranges inside indices.
     {
         std::atomic<int> bad{0};
@@ -198,14 +323,22 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
         if (bad == 3) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "BVH index outside the triangle array");
     }
 
-    cudaStream_t s = g.stream;
-    DevScene& S = g.dev;
-    S = DevScene{};
     S.triangle_count = n;
     g.triangleCount = n;
+    // The arrays built here go into one staging block and are copied as soon as each is done.
+    const size_t ngCount = n ? n : 1;
+    const size_t posCount = 3 * (indices.empty() ? 1 : indices.size());
+    const size_t pairCount = nodes.size() > 1 ? (nodes.size() - 1) / 2 : 0;
+    const size_t pairSlots = pairCount ? pairCount : 1;
+    Staging stage(s, Staging::bytesFor(ngCount * sizeof(float4)) + Staging::bytesFor(posCount * sizeof(float4)) +
+                         Staging::bytesFor(pairSlots * sizeof(NodePair)));
+    float4* ng = stage.carve<float4>(ngCount);
+    float4* pos = stage.carve<float4>(posCount);
+    NodePair* pairs = stage.carve<NodePair>(pairSlots);
     // per-triangle flags and geometric normals (Scene::accepts, geometry.cpp:282-290)
-    std::vector<float4> ng(n ? n : 1);
-    std::vector<uint32_t> flags(n ? n : 1, 0);
+    std::unique_ptr<uint32_t[]> flags(new uint32_t[ngCount]);
+    flags[0] = 0;
+    ng[0] = make_float4(0, 0, 0, 0);
     std::atomic<uint32_t> anyMaskA{0};
     std::atomic<bool> texturedEmitterA{false};
     crh::parallel_for(n, [&](uint64_t b, uint64_t e) {
@@ -250,7 +383,10 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     });
     const uint32_t anyMask = anyMaskA;
     const bool texturedEmitter = texturedEmitterA;
-    std::vector<float4> pos(3 * (indices.empty() ? 1 : indices.size()));
+    float4* devNg = g.geometry.alloc<float4>(ngCount);
+    CR_CUDA(cudaMemcpyAsync(devNg, ng, ngCount * sizeof(float4), cudaMemcpyHostToDevice, s));
+    S.tri_ng = devNg;
+    for (int k = 0; k < 3; ++k) pos[k] = make_float4(0, 0, 0, 0);
     crh::parallel_for(indices.size(), [&](uint64_t b, uint64_t e) {
         for (uint64_t slot = b; slot < e; ++slot) {
             const uint32_t idx = indices[slot];
@@ -263,8 +399,10 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
             pos[3 * slot + 2] = make_float4(t.v[2].position[0], t.v[2].position[1], t.v[2].position[2], 0.0f);
         }
     });
-    const size_t pairCount = nodes.size() > 1 ? (nodes.size() - 1) / 2 : 0;
-    std::vector<NodePair> pairs(pairCount ? pairCount : 1);
+    float4* devPos = g.geometry.alloc<float4>(posCount);
+    CR_CUDA(cudaMemcpyAsync(devPos, pos, posCount * sizeof(float4), cudaMemcpyHostToDevice, s));
+    S.tri_pos = devPos;
+    pairs[0] = NodePair{};
     auto childRef = [&](const cr_bvh_node& c, uint32_t& ref, uint32_t& cnt) {
         if (c.count) { ref = c.first; cnt = c.count; } else { ref = (c.first - 1) / 2; cnt = 0; }
     };
@@ -285,10 +423,10 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
         for (int k = 0; k < 3; ++k) { S.root_lo[k] = nodes[0].lo[k]; S.root_hi[k] = nodes[0].hi[k]; }
         childRef(nodes[0], S.root_ref, S.root_count);
     }
-    S.tri_pos = g.geometry.upload(pos.data(), pos.size(), s);
-    S.tri_ng = g.geometry.upload(ng.data(), ng.size(), s);
-    S.tris = g.geometry.upload(d.triangles, n ? n : 0, s);
-    S.pairs = g.geometry.upload(pairs.data(), pairs.size(), s);
+    NodePair* devPairs = g.geometry.alloc<NodePair>(pairSlots);
+    CR_CUDA(cudaMemcpyAsync(devPairs, pairs, pairSlots * sizeof(NodePair), cudaMemcpyHostToDevice, s));
+    S.pairs = devPairs;
+    side.join(0);  // the triangle records
     S.any_alpha_mask = anyMask;
     // A textured emitter's light sample evaluates textures, which can fail; keep it then.
     S.nee_skip = texturedEmitter ? 0u : 1u;
@@ -316,19 +454,12 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     S.image_count = d.image_count;
     S.textures = g.geometry.upload(d.textures, d.texture_count, s);
     S.texture_count = d.texture_count;
-    // environment
-    crh::EnvTables& E = g.env;
-    crh::build_environment(env, E);
+    // environment (tables and copies from the helper thread)
+    side.join(1);
     S.env_has_image = E.hasImage;
     for (int k = 0; k < 3; ++k) S.env_constant[k] = E.constant[k];
     if (E.hasImage) {
         S.env_width = E.width; S.env_height = E.height;
-        const size_t px = static_cast<size_t>(E.width) * E.height;
-        S.env_pixels = g.geometry.upload(reinterpret_cast<const float4*>(env.pixels), px, s);
-        S.env_cdf = g.geometry.upload(E.cdf.data(), E.cdf.size(), s);
-        S.env_pdf = g.geometry.upload(E.pdf.data(), E.pdf.size(), s);
-        S.env_row_cos = g.geometry.upload(E.rowCos.data(), E.rowCos.size(), s);
-        S.env_coarse = g.geometry.upload(E.coarse.data(), E.coarse.size(), s);
         S.env_coarse_count = static_cast<uint32_t>(E.coarse.size());
         S.alias_prob = nullptr;  // built on the first render that asks for alias sampling
         S.alias_index = nullptr;

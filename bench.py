@@ -54,11 +54,7 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+from replicas import Replicas, dist_env  # noqa: E402  (after the package path is set)
 
 
 class ClockSampler:
@@ -202,28 +198,20 @@ def run_reference(args):
 
 
 def run_ours(args):
-    rank, world, local = dist_env()
+    _, _, local = dist_env()
     import torch
     import crgpu
-    distributed = world > 1
-    if distributed:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    ranks = Replicas("nccl", device)
+    rank, world = ranks.rank, ranks.world
     sc, tris, nodes, idx = build_workload(args.spp)
     cam, opt = sc["camera"], sc["options"]
-    opt.seed = 42 + rank
+    opt.seed = ranks.seed(42)
     env = crgpu.env_desc(image=sc["env_image"])
     g = crgpu.GpuScene(tris, sc["materials"], env=env, bvh=(nodes, idx), device=local)
     samples_per_step = opt.width * opt.height * opt.samples
-
-    def barrier():
-        torch.cuda.synchronize(device)
-        if distributed:
-            torch.distributed.barrier()
+    barrier = ranks.barrier
 
     # counting pass (untimed): node pairs and triangles per closest-hit and any-hit ray
     tc = crgpu.Tuning()
@@ -247,12 +235,8 @@ def run_ours(args):
             barrier()
             dev_ms.append(st["device_ms"])
             launches += st["kernel_launches"]
-    total_ms = sum(dev_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
-    if distributed:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * samples_per_step * args.steps / (max_ms / 1e3) / 1e6
+    max_ms = ranks.max_over_ranks(sum(dev_ms))
+    value = ranks.whole_job_rate(samples_per_step * args.steps, max_ms / 1e3)
 
     # dominant-kernel timing: one more render with CUDA events around every launch
     tp = crgpu.Tuning()
@@ -294,10 +278,7 @@ def run_ours(args):
         ge.close()
         barrier()
         e2e_secs.append(time.perf_counter() - t0)
-    t = torch.tensor([sum(e2e_secs)], dtype=torch.float64, device=device)
-    if distributed:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * samples_per_step * args.steps / float(t.item()) / 1e6
+    e2e_value = ranks.whole_job_rate(samples_per_step * args.steps, sum(e2e_secs))
     h2d_bytes = int(tris.nbytes + nodes.nbytes + idx.nbytes + sc["env_image"].nbytes + sc["materials"].nbytes)
     d2h_bytes = int(film.nbytes)
 
@@ -327,9 +308,7 @@ def run_ours(args):
         }
         print(json.dumps(line))
     g.close()
-    if distributed:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    ranks.close()
 
 
 def mix_scenes(env_size=None, literal=False):

@@ -155,8 +155,10 @@ struct Queues {
     uint32_t* shade[kShadeClasses];  // traced paths by shading class
     uint32_t* counts;     // kCount* words
 };
+// kCountTraceWork0/1: queue entries k_trace has handed out (indexed by iteration parity);
+// kCountShadeWork0 + class: the same for each k_shade instantiation.
 enum { kCountExtend0 = 0, kCountExtend1 = 1, kCountShadow0 = 2, kCountShadow1 = 3, kCountFree0 = 4, kCountFree1 = 5,
-       kCountShade0 = 6, kCountWords = 12 };
+       kCountShade0 = 6, kCountTraceWork0 = 9, kCountShadeWork0 = 11, kCountWords = 16 };
 
 // Device error record; the host reports the one with the smallest key, which is the
 // order a single reference worker would meet them (tiles, rows, columns, samples).

@@ -12,6 +12,12 @@
 #ifndef CR_TRACE_MIN_BLOCKS
 #define CR_TRACE_MIN_BLOCKS 12
 #endif
+#ifndef CR_DYNAMIC_TRACE
+#define CR_DYNAMIC_TRACE 1
+#endif
+#ifndef CR_DYNAMIC_SHADE
+#define CR_DYNAMIC_SHADE 1
+#endif
 #ifndef CR_SHADE_MIN_BLOCKS
 #define CR_SHADE_MIN_BLOCKS 4
 #endif
@@ -95,6 +101,16 @@ CR_D void warpPush(uint32_t* queue, uint32_t* counter, bool pred, uint32_t value
 }
 
 CR_D float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// Work distribution of the queue-driven kernels: each warp takes the next 32 queue entries from
+// a counter as it becomes free, so warps whose rays finish early take more and a launch ends
+// when its work does, not when the warp with the longest fixed share does. Returns the first
+// entry of the warp's batch (all lanes get the same value).
+CR_D uint32_t warpTake(uint32_t* counter) {
+    uint32_t base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(counter, 32u);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
 
 // render.cpp:396-401 plus trace()'s initial state (render.cpp:235-239).
 CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t slot, uint32_t pixel,
@@ -574,12 +590,21 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         q.counts[kCountExtend0 + (cur ^ 1)] = 0;
         q.counts[kCountShadow0 + cur] = 0;
+        // the next iteration's counters (this iteration's shading launches follow this one)
+        q.counts[kCountTraceWork0 + (cur ^ 1)] = 0;
+        for (int c = 0; c < kShadeClasses; ++c) q.counts[kCountShadeWork0 + c] = 0;
         stats[kStatExtendRays] += nE;
         stats[kStatShadowRays] += nS;
     }
     const uint32_t total = nE + nS;
+#if CR_DYNAMIC_TRACE
+    for (uint32_t base = warpTake(&q.counts[kCountTraceWork0 + cur]); base < total;
+         base = warpTake(&q.counts[kCountTraceWork0 + cur])) {
+        const uint32_t idx = base + (threadIdx.x & 31);
+#else
     for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
         const uint32_t idx = base + threadIdx.x;
+#endif
         bool freed = false;
         int cls = -1;
         uint32_t path = 0, r = 0;
@@ -613,8 +638,14 @@ __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                                                unsigned long long* stats, JobTable J) {
     const uint32_t n = q.counts[kCountShade0 + CLASS];
     const uint32_t* in = q.shade[CLASS];
+#if CR_DYNAMIC_SHADE
+    for (uint32_t base = warpTake(&q.counts[kCountShadeWork0 + CLASS]); base < n;
+         base = warpTake(&q.counts[kCountShadeWork0 + CLASS])) {
+        const uint32_t idx = base + (threadIdx.x & 31);
+#else
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t idx = base + threadIdx.x;
+#endif
         bool cont = false, shadow = false, freed = false;
         uint32_t path = 0, r = 0;
         if (idx < n) {

@@ -164,7 +164,7 @@ CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, 
 // that ends with a queued shadow ray is finished by k_trace next iteration); freed: the path
 // ended and its slot can take a new sample. CLASS specialises the code: kShadeMiss holds only
 // environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeGeneric anything.
-template <int CLASS, bool GUIDED = false>
+template <int CLASS, bool GUIDED = false, bool LEAN = false>
 CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
                    const ErrSink& E, unsigned long long* retries, bool& cont, bool& shadow, bool& freed) {
     cont = false; shadow = false; freed = false;
@@ -199,7 +199,7 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
               static_cast<double>(kInf), t, w1, w2, det);
     const double hu = w1 / det, hv = w2 / det;
     if (medium >= 0) T = T * beerLambert(A, static_cast<float>(t));
-    const Surface s = surfaceAt(S, ray.d, tri, hu, hv, err);
+    const Surface s = surfaceAt<LEAN>(S, ray.d, tri, hu, hv, err);
     if (s.frontFace || s.doubleSided) {
         const float weight = lastDelta || !P.nee ? 1 : powerHeuristic(lastPdf, trianglePdf(S, tri, lastPosition, s.position));
         R = R + T * s.emission * weight;
@@ -229,7 +229,7 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
     if (CLASS == kShadeNeeNull && P.nee) {
         skipLight(S, rng, P.env_alias != 0);  // zero BSDF: the sample cannot contribute
     } else if (P.nee) {  // render.cpp:262-299
-        const LightSample light = sampleLight(S, s.position, rng, P.env_alias, err);
+        const LightSample light = sampleLight<LEAN>(S, s.position, rng, P.env_alias, err);
         const bool enclosedInfinite = medium >= 0 && s.thickness <= 0 && !isfin(light.distance);
         if (!enclosedInfinite && light.pdf > 0 && maxComponent(light.radiance) > 0) {
             const BsdfEval bsdf = evaluateBsdf(s, wo, light.direction);
@@ -633,7 +633,9 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
     }
 }
 
-template <int CLASS, bool MULTI = false, bool GUIDED = false>
+// LEAN (single renders of scenes without textures, punctual lights or alpha masks): the
+// shading code without those features, a smaller kernel with the same arithmetic.
+template <int CLASS, bool MULTI = false, bool GUIDED = false, bool LEAN = false>
 __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J) {
     const uint32_t n = q.counts[kCountShade0 + CLASS];
@@ -655,7 +657,7 @@ __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 shadeOne<CLASS>(*pj.S, *pj.P, pj.O, st, path, pj.E, pj.retries, cont, shadow, freed);
                 r = pj.r;
             } else {
-                shadeOne<CLASS, GUIDED>(S, P, outOf(C), st, path, E, &stats[kStatRetries], cont, shadow, freed);
+                shadeOne<CLASS, GUIDED, LEAN>(S, P, outOf(C), st, path, E, &stats[kStatRetries], cont, shadow, freed);
             }
         }
         warpPush(q.extend[cur ^ 1], &q.counts[kCountExtend0 + (cur ^ 1)], cont, path);

@@ -90,6 +90,7 @@ struct Workspace {
     uint32_t* hostCounts = nullptr;           // pinned
     unsigned long long* hostStats = nullptr;  // pinned
     int gridTrace = 0, gridShade = 0, gridShadeLight = 0, gridShadeMiss = 0, gridRegen = 0, gridSmall = 0;
+    int gridShadeLean = 0, gridShadeLightLean = 0, gridShadeMissLean = 0;
     std::vector<cudaEvent_t> events;
 
     cudaEvent_t event(size_t i) {
@@ -605,6 +606,9 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         W.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
         W.gridShadeLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
         W.gridShadeMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
+        W.gridShadeLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric, false, false, true>), 128, g.device);
+        W.gridShadeLightLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull, false, false, true>), 128, g.device);
+        W.gridShadeMissLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss, false, false, true>), 128, g.device);
         W.gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen<false>), 128, g.device);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
@@ -651,6 +655,8 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         k_pool_init<<<W.gridSmall, 128, 0, s>>>(W.q, static_cast<uint32_t>(chunkPool));
         ++launches;
         const uint64_t maxIterations = ((C.c1 - C.c0) / chunkPool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
+        // scenes without textures, punctual lights or alpha masks take the lean shading kernels
+        const bool lean = !guide && g.dev.texture_count == 0 && g.dev.punctual_count == 0 && !g.dev.any_alpha_mask;
         uint64_t iter = 0;
         int cur = 0;
         std::vector<std::pair<size_t, int>> timed;
@@ -670,6 +676,11 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                     else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                 });
+                if (lean) {
+                    rec(1, [&] { k_shade<kShadeMiss, false, false, true><<<W.gridShadeMissLean, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeNeeNull, false, false, true><<<W.gridShadeLightLean, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeGeneric, false, false, true><<<W.gridShadeLean, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                } else {
                 rec(1, [&] { k_shade<kShadeMiss><<<W.gridShadeMiss, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 rec(1, [&] { k_shade<kShadeNeeNull><<<W.gridShadeLight, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 if (guide) {
@@ -682,6 +693,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     rec(1, [&] { k_shade<kShadeGeneric, false, true><<<W.gridShade, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else {
                     rec(1, [&] { k_shade<kShadeGeneric><<<W.gridShade, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                }
                 }
                 cur ^= 1;
                 ++iter;

@@ -90,6 +90,9 @@ struct Surface {
     bool frontFace, doubleSided;
 };
 
+// LEAN: the scene has no textures (every texture slot is -1, so every lookup is exactly
+// (1, 1, 1, 1)); the instantiation leaves the texture code out of the kernel.
+template <bool LEAN = false>
 CR_D Surface surfaceAt(const DevScene& S, V3 rayDir, uint32_t tri, double hu, double hv, int& err) {
     const cr_triangle& t = S.tris[tri];
     const cr_material& material = S.materials[t.material];
@@ -109,25 +112,29 @@ CR_D Surface surfaceAt(const DevScene& S, V3 rayDir, uint32_t tri, double hu, do
     float handedness = w * t.v[0].tangent[3] + hu * t.v[1].tangent[3] + hv * t.v[2].tangent[3] < 0 ? -1.0f : 1.0f;
     s.bitangent = cross(s.normal, s.tangent) * handedness;
     float2 uv0 = make_float2(0, 0), uv1 = make_float2(0, 0);
-    const bool textured = material.base_color_texture.texture >= 0 || material.metallic_roughness_texture.texture >= 0 ||
-                          material.normal_texture.texture >= 0 || material.emissive_texture.texture >= 0 ||
-                          material.transmission_texture.texture >= 0;
-    if (textured) { uv0 = interpolateUv(t, hu, hv, 0); uv1 = interpolateUv(t, hu, hv, 1); }
-    const F4 base = sampleTexture(S, t.material, 0, uv0, uv1, true, err);
+    F4 base{1, 1, 1, 1}, mr{1, 1, 1, 1}, emissive{1, 1, 1, 1}, transmissive{1, 1, 1, 1};
+    if constexpr (!LEAN) {
+        const bool textured = material.base_color_texture.texture >= 0 || material.metallic_roughness_texture.texture >= 0 ||
+                              material.normal_texture.texture >= 0 || material.emissive_texture.texture >= 0 ||
+                              material.transmission_texture.texture >= 0;
+        if (textured) { uv0 = interpolateUv(t, hu, hv, 0); uv1 = interpolateUv(t, hu, hv, 1); }
+        base = sampleTexture(S, t.material, 0, uv0, uv1, true, err);
+        mr = sampleTexture(S, t.material, 1, uv0, uv1, false, err);
+        emissive = sampleTexture(S, t.material, 3, uv0, uv1, true, err);
+        transmissive = sampleTexture(S, t.material, 4, uv0, uv1, false, err);
+    }
     s.baseColor = V3{material.base_color[0], material.base_color[1], material.base_color[2]} * V3{base.x, base.y, base.z};
-    const F4 mr = sampleTexture(S, t.material, 1, uv0, uv1, false, err);
     s.metallic = sclamp(material.metallic * mr.z, 0.0f, 1.0f);
     s.roughness = sclamp(material.roughness * mr.y, 0.0f, 1.0f);
-    const F4 emissive = sampleTexture(S, t.material, 3, uv0, uv1, true, err);
     s.emission = v3(material.emission) * V3{emissive.x, emissive.y, emissive.z};
-    s.transmission = sclamp(material.transmission * sampleTexture(S, t.material, 4, uv0, uv1, false, err).x, 0.0f, 1.0f);
+    s.transmission = sclamp(material.transmission * transmissive.x, 0.0f, 1.0f);
     s.ior = material.ior;
     s.thickness = material.thickness;
     s.attenuationDistance = material.attenuation_distance;
     s.attenuationColor = v3(material.attenuation_color);
     s.material = t.material;
     s.doubleSided = material.double_sided != 0;
-    if (material.normal_texture.texture >= 0) {
+    if (!LEAN && material.normal_texture.texture >= 0) {
         const cr_texture_slot& slot = material.normal_texture;
         if (slot.scale[0] != 0 && slot.scale[1] != 0) {
             const double2 cs = S.slot_trig[5 * t.material + 2];
@@ -452,6 +459,8 @@ CR_D float trianglePdf(const DevScene& S, uint32_t index, V3 from, V3 point) {
     const float len2 = lengthSquared(dir), cosine = fabsf(dot(v3(t.geometric_normal), normalize(dir)));
     return cosine > 1e-8f ? __ldg(S.tri_light_probability + index) * len2 / (t.area * cosine) : 0;
 }
+// LEAN: besides having no textures, the scene has no punctual lights and no alpha masks.
+template <bool LEAN = false>
 CR_D LightSample sampleLight(const DevScene& S, V3 from, Rng& rng, bool alias, int& err) {
     LightSample out = emptyLight();
     if (S.light_entry_count == 0) return out;
@@ -469,7 +478,7 @@ CR_D LightSample sampleLight(const DevScene& S, V3 from, Rng& rng, bool alias, i
         out.radiance = envRadiance(S, out.direction);
         return out;
     }
-    if (e.type == kLightPunctual) {
+    if (!LEAN && e.type == kLightPunctual) {
         const DevPunctual& l = S.punctual[e.index];
         out.delta = true; out.pdf = e.probability;
         float attenuation = 1;
@@ -504,8 +513,8 @@ CR_D LightSample sampleLight(const DevScene& S, V3 from, Rng& rng, bool alias, i
     // Scene::accepts on Ray{from, direction} with Hit{distance, u1, u2}
     const uint32_t flags = __float_as_uint(__ldg(S.tri_ng + e.index).w);
     if ((flags & kTriCull) && !accepts_cull(S, e.index, out.direction)) return emptyLight();
-    if ((flags & kTriAlphaMask) && !accepts_alpha(S, e.index, u1, u2)) return emptyLight();
-    const Surface s = surfaceAt(S, out.direction, e.index, u1, u2, err);
+    if (!LEAN && (flags & kTriAlphaMask) && !accepts_alpha(S, e.index, u1, u2)) return emptyLight();
+    const Surface s = surfaceAt<LEAN>(S, out.direction, e.index, u1, u2, err);
     if (!s.frontFace && !s.doubleSided) return emptyLight();
     out.radiance = s.emission;
     out.pdf = trianglePdf(S, e.index, from, out.target);

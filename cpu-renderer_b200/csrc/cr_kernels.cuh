@@ -415,7 +415,7 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
 
 // Any hit for one queued shadow ray; an unoccluded contribution is added (render.cpp:283-296).
 // Returns true when the path had ended and its slot is now free.
-template <bool COUNT = false>
+template <bool COUNT = false, bool NOALPHA = false>
 CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
                     const ErrSink& E, unsigned long long* stats = nullptr) {
     const float4 o = st.sh_o[path], d = st.sh_d[path], lo = st.sh_lo[path], c = st.sh_c[path];
@@ -425,7 +425,7 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
     h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
     int err = 0;
     VisitCount vc;
-    const bool blocked = intersect<true, COUNT>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0,
+    const bool blocked = intersect<true, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0,
                                                 h, err, &vc);
     if (err) raise(E, P, st.pixel[path], st.sample[path], err);
     if (COUNT) {
@@ -442,7 +442,7 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
     return false;
 }
 
-template <bool COUNT>
+template <bool COUNT, bool NOALPHA = false>
 CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
                     unsigned long long* stats) {
     const uint32_t flags = st.flags[path];
@@ -451,7 +451,7 @@ CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st,
     h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
     int err = 0;
     VisitCount vc;
-    const bool found = intersect<false, COUNT>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
+    const bool found = intersect<false, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
                                                h, err, &vc);
     st.hit_tri[path] = found ? h.tri : kNoTriangle;
     if (st.guide.hitT) st.guide.hitT[path] = found ? static_cast<float>(h.t) : 0.0f;
@@ -582,7 +582,8 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
 }
 
 // Closest hit for the live queue and any hit for last iteration's shadow rays, one launch.
-template <bool COUNT, bool MULTI = false>
+// NOALPHA: the scene has no alpha-masked triangles (single renders), see accepts<NOALPHA>.
+template <bool COUNT, bool MULTI = false, bool NOALPHA = false>
 __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J) {
     const uint32_t nE = q.counts[kCountExtend0 + cur];
@@ -614,7 +615,7 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
                 const PathJob pj = pathJob(J, path);
                 cls = closestOne<COUNT>(*pj.S, *pj.P, st, path, pj.E, stats);
             } else {
-                cls = closestOne<COUNT>(S, P, st, path, E, stats);
+                cls = closestOne<COUNT, NOALPHA>(S, P, st, path, E, stats);
             }
         } else if (idx < total) {
             path = q.shadow[cur ^ 1][idx - nE];
@@ -623,7 +624,7 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
                 freed = shadowOne<COUNT>(*pj.S, *pj.P, pj.O, st, path, pj.E, stats);
                 r = pj.r;
             } else {
-                freed = shadowOne<COUNT>(S, P, outOf(C), st, path, E, stats);
+                freed = shadowOne<COUNT, NOALPHA>(S, P, outOf(C), st, path, E, stats);
             }
         }
         warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);

@@ -90,7 +90,7 @@ struct Workspace {
     uint32_t* hostCounts = nullptr;           // pinned
     unsigned long long* hostStats = nullptr;  // pinned
     int gridTrace = 0, gridShade = 0, gridShadeLight = 0, gridShadeMiss = 0, gridRegen = 0, gridSmall = 0;
-    int gridShadeLean = 0, gridShadeLightLean = 0, gridShadeMissLean = 0;
+    int gridShadeLean = 0, gridShadeLightLean = 0, gridShadeMissLean = 0, gridTraceNoAlpha = 0;
     std::vector<cudaEvent_t> events;
 
     cudaEvent_t event(size_t i) {
@@ -606,6 +606,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         W.gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
         W.gridShadeLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
         W.gridShadeMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
+        W.gridTraceNoAlpha = occupancyGrid(reinterpret_cast<const void*>(k_trace<false, false, true>), 128, g.device);
         W.gridShadeLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric, false, false, true>), 128, g.device);
         W.gridShadeLightLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull, false, false, true>), 128, g.device);
         W.gridShadeMissLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss, false, false, true>), 128, g.device);
@@ -657,6 +658,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         const uint64_t maxIterations = ((C.c1 - C.c0) / chunkPool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
         // scenes without textures, punctual lights or alpha masks take the lean shading kernels
         const bool lean = !guide && g.dev.texture_count == 0 && g.dev.punctual_count == 0 && !g.dev.any_alpha_mask;
+        const bool noAlpha = !g.dev.any_alpha_mask;
         uint64_t iter = 0;
         int cur = 0;
         std::vector<std::pair<size_t, int>> timed;
@@ -674,6 +676,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                 rec(2, [&] { k_regen<false><<<W.gridRegen, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
                 rec(0, [&] {
                     if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    else if (noAlpha) k_trace<false, false, true><<<W.gridTraceNoAlpha, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                     else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                 });
                 if (lean) {

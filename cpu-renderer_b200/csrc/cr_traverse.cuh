@@ -87,9 +87,12 @@ CR_D bool accepts_cull(const DevScene& S, uint32_t tri, V3 dir) {
 // Implemented in cr_shade.cuh (needs the texture sampler).
 CR_D bool accepts_alpha(const DevScene& S, uint32_t tri, double u, double v);
 
+// NOALPHA: the scene has no alpha-masked triangle (no kTriAlphaMask flag is set), so the
+// instantiation leaves the texture lookup of the alpha test out of the traversal.
+template <bool NOALPHA = false>
 CR_D bool accepts(const DevScene& S, uint32_t tri, uint32_t flags, V3 dir, double w1, double w2, double det) {
     if ((flags & kTriCull) && !accepts_cull(S, tri, dir)) return false;
-    if (flags & kTriAlphaMask) return accepts_alpha(S, tri, w1 / det, w2 / det);
+    if (!NOALPHA && (flags & kTriAlphaMask)) return accepts_alpha(S, tri, w1 / det, w2 / det);
     return true;
 }
 
@@ -103,7 +106,7 @@ CR_D void load_pair(const NodePair* pairs, uint32_t p, float4& a, float4& b, flo
 // Optional visit counters (node pairs fetched, triangles tested) for the roofline numerator.
 struct VisitCount { uint32_t pairs = 0, tris = 0; };
 
-template <bool ANY, bool COUNT = false>
+template <bool ANY, bool COUNT = false, bool NOALPHA = false>
 __device__ bool intersect_exact(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore,
                                 HitRec& hit, int& err, VisitCount* vc = nullptr) {
     double closestLimit = smin(static_cast<double>(ray.tmax), hitT);
@@ -163,7 +166,7 @@ __device__ bool intersect_exact(const DevScene& S, const TRay& ray, double hitT,
                 if (limit < ray.tmin) continue;
                 double t, w1, w2, det;
                 if (!tri_exact(E, v3(q0), v3(q1), v3(q2), ray.tmin, limit, t, w1, w2, det)) continue;
-                if (!accepts(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
+                if (!accepts<NOALPHA>(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
                 if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; hit.flags = __float_as_uint(q1.w); return true; }
                 if (!found || t < hit.t || (t == hit.t && index < hit.tri)) {
                     hit.t = t; hit.tri = index; hit.flags = __float_as_uint(q1.w); bestW1 = w1; bestW2 = w2; bestDet = det;
@@ -298,7 +301,7 @@ CR_D bool tri_reject_fast(const FastSetup& F, float4 p0, float4 p1, float4 p2) {
 // postpones the first leaf it reaches, continuing speculatively until every lane of the warp
 // holds a leaf; then all lanes test their leaf's triangles together. Lanes therefore run the
 // node code and the triangle code in separate loops instead of alternating per iteration.
-template <bool ANY, bool COUNT = false>
+template <bool ANY, bool COUNT = false, bool NOALPHA = false>
 __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore,
                                HitRec& hit, int& err, VisitCount* vc = nullptr) {
     double closestLimit = smin(static_cast<double>(ray.tmax), hitT);
@@ -358,7 +361,7 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
             if (limit < ray.tmin) continue;
             double t, w1, w2, det;
             if (!tri_exact(E, v3(q0), v3(q1), v3(q2), ray.tmin, limit, t, w1, w2, det)) continue;
-            if (!accepts(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
+            if (!accepts<NOALPHA>(S, index, __float_as_uint(q1.w), ray.d, w1, w2, det)) continue;
             if (ANY) { hit.t = t; hit.u = w1 / det; hit.v = w2 / det; hit.tri = index; hit.flags = __float_as_uint(q1.w); return true; }
             if (!found || t < hit.t || (t == hit.t && index < hit.tri)) {
                 hit.t = t; hit.tri = index; hit.flags = __float_as_uint(q1.w); bestW1 = w1; bestW2 = w2; bestDet = det;
@@ -375,12 +378,12 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
 
 // Bvh::intersect entry: the reference's preconditions (geometry.cpp:555), then the traversal
 // that fits the ray.
-template <bool ANY, bool COUNT = false>
+template <bool ANY, bool COUNT = false, bool NOALPHA = false>
 __device__ bool intersect(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore, bool forceExact,
                           HitRec& hit, int& err, VisitCount* vc = nullptr) {
     if (!S.has_root || !validRay(ray) || isnan(hitT)) return false;
-    if (forceExact || !fast_eligible(ray)) return intersect_exact<ANY, COUNT>(S, ray, hitT, ignore, hit, err, vc);
-    return intersect_fast<ANY, COUNT>(S, ray, hitT, ignore, hit, err, vc);
+    if (forceExact || !fast_eligible(ray)) return intersect_exact<ANY, COUNT, NOALPHA>(S, ray, hitT, ignore, hit, err, vc);
+    return intersect_fast<ANY, COUNT, NOALPHA>(S, ray, hitT, ignore, hit, err, vc);
 }
 
 }  // namespace crg

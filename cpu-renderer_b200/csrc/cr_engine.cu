@@ -178,7 +178,7 @@ class Engine {
     ~Engine() {
         cudaSetDevice(device_);
         if (s_) cudaStreamSynchronize(s_);
-        if (graph_) cudaGraphExecDestroy(graph_);
+        for (auto& g : graph_) if (g) cudaGraphExecDestroy(g);
         for (auto& a : active_) a.buffers.release();
         pool_.release();
         scratchAlloc_.release();
@@ -255,7 +255,50 @@ class Engine {
         std::lock_guard<std::mutex> lock(mutex_);
         cr_engine_stats s = stats_host_;
         s.seconds = busySeconds_;
+        s.extend_rays += solo_.extend_rays;
+        s.shadow_rays += solo_.shadow_rays;
         return s;
+    }
+
+    // Registers a job that will render alone (it never enters the pending queue): its ticket.
+    uint64_t registerSolo(cr_job* j) {
+        std::lock_guard<std::mutex> lock(mutex_);
+        j->submitted_at = now();
+        j->started_at = j->first_frame_at = j->finished_at = 0;
+        j->status = CR_OK;
+        j->error[0] = 0;
+        std::memset(&j->stats, 0, sizeof(j->stats));
+        return ++lastTicket_;
+    }
+
+    // A batch job that fills the pool on its own renders alone through the single-render entry
+    // points: its rays then stay in its own sample order (the pool holds no other job's paths)
+    // and the kernels can be the lean variants its scene allows. Its times, status and stats
+    // are kept as for a pooled job. Runs on its own host thread beside step().
+    void runSolo(cr_job* j, uint64_t ticket) {
+        j->started_at = now();
+        struct Hook {
+            Engine* e;
+            cr_job* j;
+            static void frame(uint32_t spp, const void* data, uint64_t size, void* user) {
+                Hook* h = static_cast<Hook*>(user);
+                if (!h->j->first_frame_at) h->j->first_frame_at = h->e->now();
+                if (h->j->on_frame) h->j->on_frame(spp, data, size, h->j->user);
+            }
+        } hook{this, j};
+        const cr_status st = j->every_samples
+            ? cr_gpu_render_progressive(j->scene, &j->camera, &j->options, j->every_samples, j->format, j->exposure,
+                                        &Hook::frame, &hook, j->film_rgb, &j->stats, nullptr)
+            : cr_gpu_render(j->scene, &j->camera, &j->options, nullptr, nullptr, j->film_rgb, &j->stats, nullptr);
+        char message[sizeof(j->error)] = {0};
+        if (st != CR_OK) cr_gpu_last_error(message, sizeof(message));
+        endJob(j, ticket, st, message);
+        std::lock_guard<std::mutex> lock(mutex_);
+        if (st == CR_OK) stats_host_.camera_samples += j->stats.camera_samples;
+        stats_host_.iterations += j->stats.iterations;
+        stats_host_.launches += j->stats.kernel_launches;
+        solo_.extend_rays += j->stats.extend_rays;
+        solo_.shadow_rays += j->stats.shadow_rays;
     }
     int device() const { return device_; }
 
@@ -409,27 +452,46 @@ class Engine {
         hCtl_[0] = issueEnd_;
         hCtl_[1] = rangeCount_;
         CR_CUDA(cudaMemcpyAsync(ctl_, hCtl_, 2 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s_));
+        // Kernel variant: without the alpha test when no active job's scene has alpha-masked
+        // triangles, lean shading when none has textures, punctual lights or alpha masks (a job's
+        // paths leave the pool before it ends, so only active jobs' paths are traced or shaded).
+        bool noAlpha = true, lean = true;
+        for (const Active& a : active_) {
+            const DevScene& S = a.job->scene->dev;
+            noAlpha = noAlpha && !S.any_alpha_mask;
+            lean = lean && !S.any_alpha_mask && S.texture_count == 0 && S.punctual_count == 0;
+        }
+        const int variant = (noAlpha ? 1 : 0) | (lean ? 2 : 0);
         if (cfg_.graphs) {
-            if (!graph_) {
+            if (!graph_[variant]) {
                 cudaGraph_t g = nullptr;
                 CR_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-                launchIterations();
+                launchIterations(variant);
                 CR_CUDA(cudaStreamEndCapture(s_, &g));
-                CR_CUDA(cudaGraphInstantiate(&graph_, g, 0));
+                CR_CUDA(cudaGraphInstantiate(&graph_[variant], g, 0));
                 cudaGraphDestroy(g);
             }
-            CR_CUDA(cudaGraphLaunch(graph_, s_));
+            CR_CUDA(cudaGraphLaunch(graph_[variant], s_));
             std::lock_guard<std::mutex> lock(mutex_);
             ++stats_host_.graph_steps;
         } else {
-            launchIterations();
+            launchIterations(variant);
         }
         std::lock_guard<std::mutex> lock(mutex_);
         stats_host_.iterations += cfg_.iters;
         stats_host_.launches += 5ull * cfg_.iters;
     }
 
-    void launchIterations() {
+    void launchIterations(int variant) {
+        switch (variant) {
+            case 0: launchIterationsT<false, false>(); break;
+            case 1: launchIterationsT<true, false>(); break;
+            default: launchIterationsT<true, true>(); break;  // lean implies no alpha masks
+        }
+    }
+
+    template <bool NOALPHA, bool LEAN>
+    void launchIterationsT() {
         const DevScene S{};
         const RenderParams P{};
         const Chunk C{};
@@ -438,10 +500,10 @@ class Engine {
             const int cur = static_cast<int>(i & 1);
             const int refill = (i % cfg_.refill) == 0;
             k_regen<true><<<gridRegen_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_, refill);
-            k_trace<false, true><<<gridTrace_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
-            k_shade<kShadeMiss, true><<<gridMiss_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
-            k_shade<kShadeNeeNull, true><<<gridLight_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
-            k_shade<kShadeGeneric, true><<<gridShade_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_trace<false, true, NOALPHA><<<gridTrace_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_shade<kShadeMiss, true, false, LEAN><<<gridMiss_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_shade<kShadeNeeNull, true, false, LEAN><<<gridLight_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_shade<kShadeGeneric, true, false, LEAN><<<gridShade_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
         }
         CR_CUDA(cudaGetLastError());
     }
@@ -598,7 +660,7 @@ class Engine {
     std::vector<DevScene> hScenes_;
     std::vector<RenderParams> hParams_;
     int gridTrace_ = 0, gridShade_ = 0, gridLight_ = 0, gridMiss_ = 0, gridRegen_ = 0, gridSmall_ = 0;
-    cudaGraphExec_t graph_ = nullptr;
+    cudaGraphExec_t graph_[4] = {};  // one per kernel variant (bit 0: no alpha test, bit 1: lean shading)
     // issue list state
     uint32_t rangeCount_ = 0, uploaded_ = 0, firstOpen_ = 0;
     uint64_t openRanges_ = 0, issueEnd_ = 0, issuedPos_ = 0, live_ = 0;
@@ -614,6 +676,7 @@ class Engine {
     std::map<uint64_t, cr_status> ended_;
     uint64_t lastTicket_ = 0;
     cr_engine_stats stats_host_{};
+    cr_engine_stats solo_{};  // rays of the jobs rendered alone (the pool's own come from the device)
     double busySeconds_ = 0;
 };
 
@@ -629,6 +692,8 @@ struct cr_server {
 
 namespace {
 
+constexpr uint32_t kSoloSamplesLog2 = 24;
+
 cr_status runBatch(cr_job* jobs, uint32_t count, const cr_engine_tuning* tuning, cr_engine_stats* stats) {
     if (count == 0) {
         if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -640,14 +705,51 @@ cr_status runBatch(cr_job* jobs, uint32_t count, const cr_engine_tuning* tuning,
         if (jobs[i].scene) { device = jobs[i].scene->device; break; }
     if (device < 0) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "no job has a scene");
     Engine e(device, tuning, 1);
-    for (uint32_t i = 0; i < count; ++i) e.submit(&jobs[i]);
+    // Jobs of at least 2^solo camera samples fill the pool on their own: they render alone, in
+    // order, before the pool takes the rest.
+    const uint32_t soloLog2 = tuning && tuning->solo_samples_log2 ? tuning->solo_samples_log2 : kSoloSamplesLog2;
+    const auto wall0 = std::chrono::steady_clock::now();
+    std::vector<std::pair<cr_job*, uint64_t>> solo;
+    for (uint32_t i = 0; i < count; ++i) {
+        const cr_job& j = jobs[i];
+        const cr_render_options& o = j.options;
+        const uint64_t total = o.width > 0 && o.height > 0 && o.samples > 0
+                                   ? static_cast<uint64_t>(o.width) * static_cast<uint64_t>(o.height) * static_cast<uint64_t>(o.samples)
+                                   : 0;
+        if (soloLog2 < 64 && j.scene && j.scene->device == device && total >= (uint64_t{1} << soloLog2))
+            solo.push_back({&jobs[i], e.registerSolo(&jobs[i])});
+        else
+            e.submit(&jobs[i]);
+    }
+    // The solo renders run on a helper thread (on their scenes' streams) while this thread steps
+    // the pool (on the engine's stream): the pool's kernels fill the device when a solo render's
+    // launches drain.
+    std::exception_ptr soloError;
+    std::thread soloThread([&] {
+        try {
+            CR_CUDA(cudaSetDevice(device));
+            for (auto& [j, ticket] : solo) e.runSolo(j, ticket);
+        } catch (...) {
+            soloError = std::current_exception();
+        }
+    });
+    struct Join {
+        std::thread& t;
+        ~Join() { if (t.joinable()) t.join(); }
+    } join{soloThread};
     try {
         while (!e.idle()) e.step();
     } catch (const std::exception& ex) {
         e.failAll(CR_ERR_CUDA, ex.what());
         throw;
     }
-    if (stats) *stats = e.stats();
+    soloThread.join();
+    if (soloError) std::rethrow_exception(soloError);
+    if (stats) {
+        *stats = e.stats();
+        if (!solo.empty())  // the pool and the solo renders overlap: the batch's wall time
+            stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+    }
     for (uint32_t i = 0; i < count; ++i)
         if (jobs[i].status != CR_OK) return crh::set_last_error(jobs[i].status, jobs[i].error);
     return CR_OK;
@@ -666,7 +768,18 @@ cr_status cr_gpu_render_batch(cr_job* jobs, uint32_t count, const cr_engine_tuni
 cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tuning* tuning) {
     try {
         if (!jobs || !tuning || count == 0) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
-        std::vector<cr_job> trial(jobs, jobs + count);
+        // the jobs that will share the pool (larger ones render alone, see runBatch) at 1 spp
+        const uint32_t soloLog2 = tuning->solo_samples_log2 ? tuning->solo_samples_log2 : kSoloSamplesLog2;
+        std::vector<cr_job> trial;
+        for (uint32_t i = 0; i < count; ++i) {
+            const cr_render_options& o = jobs[i].options;
+            const uint64_t total = o.width > 0 && o.height > 0 && o.samples > 0
+                                       ? static_cast<uint64_t>(o.width) * static_cast<uint64_t>(o.height) * static_cast<uint64_t>(o.samples)
+                                       : 0;
+            if (soloLog2 < 64 && jobs[i].scene && total >= (uint64_t{1} << soloLog2)) continue;
+            trial.push_back(jobs[i]);
+        }
+        if (trial.empty()) return CR_OK;
         for (auto& j : trial) {
             j.options.samples = 1;
             j.film_rgb = nullptr;
@@ -685,11 +798,13 @@ cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tu
                 t.refill_free_percent = pct;
                 t.iterations_per_step = 8;
                 const auto t0 = std::chrono::steady_clock::now();
-                const cr_status st = runBatch(trial.data(), count, &t, nullptr);
+                t.solo_samples_log2 = 64;  // the trial jobs are the pool's
+                const cr_status st = runBatch(trial.data(), static_cast<uint32_t>(trial.size()), &t, nullptr);
                 const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
                 if (st != CR_OK) return st;
                 if (sec < bestSeconds) { bestSeconds = sec; best = t; }
             }
+        best.solo_samples_log2 = tuning->solo_samples_log2;  // the trials ran the pool's jobs only
         *tuning = best;
         return CR_OK;
     } catch (const std::exception& e) { return fail(e); }

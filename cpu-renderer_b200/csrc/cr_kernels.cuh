@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
 }
 
 // Closest hit for the live queue and any hit for last iteration's shadow rays, one launch.
-// NOALPHA: the scene has no alpha-masked triangles (single renders), see accepts<NOALPHA>.
+// NOALPHA: no scene whose paths the launch traces has alpha-masked triangles, see accepts<NOALPHA>.
 template <bool COUNT, bool MULTI = false, bool NOALPHA = false>
 __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J) {
@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
             path = q.extend[cur][idx];
             if constexpr (MULTI) {
                 const PathJob pj = pathJob(J, path);
-                cls = closestOne<COUNT>(*pj.S, *pj.P, st, path, pj.E, stats);
+                cls = closestOne<COUNT, NOALPHA>(*pj.S, *pj.P, st, path, pj.E, stats);
             } else {
                 cls = closestOne<COUNT, NOALPHA>(S, P, st, path, E, stats);
             }
@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
             path = q.shadow[cur ^ 1][idx - nE];
             if constexpr (MULTI) {
                 const PathJob pj = pathJob(J, path);
-                freed = shadowOne<COUNT>(*pj.S, *pj.P, pj.O, st, path, pj.E, stats);
+                freed = shadowOne<COUNT, NOALPHA>(*pj.S, *pj.P, pj.O, st, path, pj.E, stats);
                 r = pj.r;
             } else {
                 freed = shadowOne<COUNT, NOALPHA>(S, P, outOf(C), st, path, E, stats);
@@ -634,8 +634,8 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
     }
 }
 
-// LEAN (single renders of scenes without textures, punctual lights or alpha masks): the
-// shading code without those features, a smaller kernel with the same arithmetic.
+// LEAN (every scene whose paths the launch shades has no textures, punctual lights or alpha
+// masks): the shading code without those features, a smaller kernel with the same arithmetic.
 template <int CLASS, bool MULTI = false, bool GUIDED = false, bool LEAN = false>
 __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J) {
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
             path = in[idx];
             if constexpr (MULTI) {
                 const PathJob pj = pathJob(J, path);
-                shadeOne<CLASS>(*pj.S, *pj.P, pj.O, st, path, pj.E, pj.retries, cont, shadow, freed);
+                shadeOne<CLASS, false, LEAN>(*pj.S, *pj.P, pj.O, st, path, pj.E, pj.retries, cont, shadow, freed);
                 r = pj.r;
             } else {
                 shadeOne<CLASS, GUIDED, LEAN>(S, P, outOf(C), st, path, E, &stats[kStatRetries], cont, shadow, freed);

@@ -473,7 +473,10 @@ typedef struct cr_engine_tuning {
     uint64_t memory_budget;       /* bytes of job buffers admitted at once; 0: 150 GB          */
     uint32_t refill_free_percent; /* refill only when at least this share of the pool is free
                                      (new paths then start together, as one wave); 0: always   */
-    uint32_t reserved;
+    uint32_t solo_samples_log2;   /* cr_gpu_render_batch: a job of at least 2^n camera samples
+                                     fills the pool on its own and renders alone (the single-
+                                     render path), before the pool takes the rest; 0: n = 24;
+                                     64 or more: every job shares the pool. Servers ignore it  */
 } cr_engine_tuning;
 
 typedef struct cr_engine_stats {

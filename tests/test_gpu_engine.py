@@ -80,6 +80,35 @@ def test_batch_films_equal_single_renders(crgpu, world, tuning):
         assert stats["graph_steps"] > 0
 
 
+def test_batch_solo_jobs(crgpu, world):
+    """Jobs of at least 2^solo_samples_log2 samples render alone through the single-render path
+    (here 2^14: the 64x48x16, 160x90x4 and 128x128x2 jobs), the rest share the pool; every film,
+    status and sample count is the standalone render's, and progressive frames and failures
+    of solo jobs are reported as for pooled ones."""
+    jobs = _mixed_jobs(crgpu, world)
+    frames = JobSpec(world["room"], world["room_cam"], _opts(crgpu, 64, 64, 8), every=4, fmt=1)
+    bad_cam = crgpu.Camera.make(position=(20, -0.5, 0), forward=(0, 1, 0), right=(1, 0, 0), up=(0, 0, 1), yfov=1e-7)
+    failing = JobSpec(world["touch"], bad_cam, _opts(crgpu, 128, 128, 8, bounces=8))
+    jobs += [frames, failing]
+    stats = render_batch(jobs, EngineTuning.make(pool_paths=8192, range_samples=3000, solo_samples_log2=14))
+    assert stats["jobs_done"] == len(jobs) - 1 and stats["jobs_failed"] == 1
+    assert stats["camera_samples"] == sum(j.stats["camera_samples"] for j in jobs[:-1])
+    for i, j in enumerate(jobs[:-1]):
+        assert j.status == 0, j.error
+        film, st = _alone(j)
+        assert np.array_equal(j.film, film), f"job {i}"
+        assert j.stats["camera_samples"] == st["camera_samples"]
+        assert j.times["finished"] >= j.times["started"] >= j.times["submitted"]
+    assert [s for s, _ in frames.frames] == [4, 8]
+    for done, data in frames.frames:
+        film, _ = frames.scene.render(frames.camera, _opts(crgpu, 64, 64, done))
+        assert data == oracle.encode(film, 1, 0.0), done
+    assert frames.times["first_frame"] > 0
+    with pytest.raises(crgpu.CrError) as e:
+        failing.scene.render(failing.camera, failing.options)
+    assert failing.status == e.value.status and failing.error == str(e.value)
+
+
 def test_batch_progressive_frames(crgpu, world):
     jobs = [JobSpec(world["room"], world["room_cam"], _opts(crgpu, 40, 30, 10), every=4, fmt=0, exposure=0.5),
             JobSpec(world["grid"], world["grid_cam"], _opts(crgpu, 64, 36, 6, seed=3), every=2, fmt=2),

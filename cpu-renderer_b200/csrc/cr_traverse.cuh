@@ -260,8 +260,10 @@ CR_D bool box_fast(const FastSetup& F, float lx, float ly, float lz, float hx, f
     }
     float tn = fmaxf(fmaxf(nx, ny), nz);
     float tf = fminf(fminf(fx, fy), fz);
-    tn = tn - fabsf(tn) * kBoxRel - kBoxAbs;
-    tf = tf + fabsf(tf) * kBoxRel + kBoxAbs;
+    // one rounding fewer than tn - |tn| kBoxRel: the widening needs ~0.2 of its 2^-20, so how
+    // its own product rounds does not matter
+    tn = __fmaf_rn(-fabsf(tn), kBoxRel, tn) - kBoxAbs;
+    tf = __fmaf_rn(fabsf(tf), kBoxRel, tf) + kBoxAbs;
     tn = fmaxf(tn, tmin);
     tf = fminf(tf, tmax);
     tnear = tn;

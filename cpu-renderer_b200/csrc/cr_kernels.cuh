@@ -8,7 +8,8 @@
 
 // Minimum resident blocks per SM requested from the register allocator (128-thread blocks).
 // k_trace at 12 (40 registers, some spills to L1) measured ~2 % faster than at 8 or 10 on
-// the 1M-triangle workload; k_shade above 4 loses more to spills than it gains.
+// the 1M-triangle workload; k_shade above 4 loses more to spills than it gains (also per
+// class: the NEE-null kernel at 5, 6 or 8 and the miss kernel at 8 measured slower).
 #ifndef CR_TRACE_MIN_BLOCKS
 #define CR_TRACE_MIN_BLOCKS 12
 #endif

@@ -657,7 +657,11 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         ++launches;
         const uint64_t maxIterations = ((C.c1 - C.c0) / chunkPool + 3) * 2 * static_cast<uint64_t>(o.bounces + 2) + 16;
         // scenes without textures, punctual lights or alpha masks take the lean shading kernels
-        const bool lean = !guide && g.dev.texture_count == 0 && g.dev.punctual_count == 0 && !g.dev.any_alpha_mask;
+        const bool lean = g.dev.texture_count == 0 && g.dev.punctual_count == 0 && !g.dev.any_alpha_mask;
+        // no launch needs more blocks than the chunk's pool has 128-path batches (warps take
+        // their batches from a counter, so a smaller grid only spares the launch its idle blocks)
+        const int poolBlocks = static_cast<int>(std::min<uint64_t>((chunkPool + 127) / 128, 1u << 30));
+        auto cap = [&](int grid) { return std::max(1, std::min(grid, poolBlocks)); };
         const bool noAlpha = !g.dev.any_alpha_mask;
         uint64_t iter = 0;
         int cur = 0;
@@ -673,19 +677,20 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     if (timePhases) { CR_CUDA(cudaEventRecord(W.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
                     ++launches;
                 };
-                rec(2, [&] { k_regen<false><<<W.gridRegen, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
+                rec(2, [&] { k_regen<false><<<cap(W.gridRegen), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
                 rec(0, [&] {
-                    if (tuning.count_traversal) k_trace<true><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                    else if (noAlpha) k_trace<false, false, true><<<W.gridTraceNoAlpha, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                    else k_trace<false><<<W.gridTrace, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    if (tuning.count_traversal) k_trace<true><<<cap(W.gridTrace), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    else if (noAlpha) k_trace<false, false, true><<<cap(W.gridTraceNoAlpha), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    else k_trace<false><<<cap(W.gridTrace), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                 });
+                // shading: the lean instantiations when the scene allows them
                 if (lean) {
-                    rec(1, [&] { k_shade<kShadeMiss, false, false, true><<<W.gridShadeMissLean, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
-                    rec(1, [&] { k_shade<kShadeNeeNull, false, false, true><<<W.gridShadeLightLean, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
-                    rec(1, [&] { k_shade<kShadeGeneric, false, false, true><<<W.gridShadeLean, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else {
-                rec(1, [&] { k_shade<kShadeMiss><<<W.gridShadeMiss, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
-                rec(1, [&] { k_shade<kShadeNeeNull><<<W.gridShadeLight, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                }
                 if (guide) {
                     rec(1, [&] {
                         guideInferPaths(guide->gd, s, W.q.shade[kShadeGeneric], W.q.counts + kCountShade0 + kShadeGeneric,
@@ -693,10 +698,12 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                                         V3{st.guide.lo[0], st.guide.lo[1], st.guide.lo[2]},
                                         V3{st.guide.inv[0], st.guide.inv[1], st.guide.inv[2]}, guideOut);
                     });
-                    rec(1, [&] { k_shade<kShadeGeneric, false, true><<<W.gridShade, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    if (lean) rec(1, [&] { k_shade<kShadeGeneric, false, true, true><<<cap(W.gridShadeLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    else rec(1, [&] { k_shade<kShadeGeneric, false, true><<<cap(W.gridShade), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                } else if (lean) {
+                    rec(1, [&] { k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else {
-                    rec(1, [&] { k_shade<kShadeGeneric><<<W.gridShade, 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
-                }
+                    rec(1, [&] { k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 }
                 cur ^= 1;
                 ++iter;

@@ -414,6 +414,32 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
     cont = true;
 }
 
+// What follows a shadow ray's any-hit query: an unoccluded contribution c is added to the
+// path's radiance (render.cpp:283-296). Returns true when the path had ended and its slot is
+// now free.
+CR_D bool shadowFinish(const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path, const ErrSink& E,
+                       bool blocked, int err, float4 c) {
+    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    const float4 ra = st.rad[path];
+    V3 R = v3(ra);
+    if (!blocked) R = R + v3(c);
+    if (st.guide.count) guideNeeResolved(st.guide, path, blocked ? V3{} : v3(c));
+    const uint32_t flags = st.flags[path];
+    if (flags & kPathDead) { finishPath(P, O, st, path, R, E); return true; }
+    st.rad[path] = f4(R, ra.w);
+    return false;
+}
+
+// What follows a path's closest-hit query: the hit is recorded and its shading class returned.
+CR_D int closestFinish(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
+                       bool found, const HitRec& h, int err) {
+    st.hit_tri[path] = found ? h.tri : kNoTriangle;
+    if (st.guide.hitT) st.guide.hitT[path] = found ? static_cast<float>(h.t) : 0.0f;
+    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
+    if (!found) return kShadeMiss;
+    return (S.nee_skip && (h.flags & kTriNeeNull)) ? kShadeNeeNull : kShadeGeneric;
+}
+
 // Any hit for one queued shadow ray; an unoccluded contribution is added (render.cpp:283-296).
 // Returns true when the path had ended and its slot is now free.
 template <bool COUNT = false, bool NOALPHA = false>
@@ -428,19 +454,11 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
     VisitCount vc;
     const bool blocked = intersect<true, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), __float_as_uint(lo.w), P.exact_traversal != 0,
                                                 h, err, &vc);
-    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
     if (COUNT) {
         atomicAdd(&stats[kStatShadowPairs], static_cast<unsigned long long>(vc.pairs));
         atomicAdd(&stats[kStatShadowTris], static_cast<unsigned long long>(vc.tris));
     }
-    const float4 ra = st.rad[path];
-    V3 R = v3(ra);
-    if (!blocked) R = R + v3(c);
-    if (st.guide.count) guideNeeResolved(st.guide, path, blocked ? V3{} : v3(c));
-    const uint32_t flags = st.flags[path];
-    if (flags & kPathDead) { finishPath(P, O, st, path, R, E); return true; }
-    st.rad[path] = f4(R, ra.w);
-    return false;
+    return shadowFinish(P, O, st, path, E, blocked, err, c);
 }
 
 template <bool COUNT, bool NOALPHA = false>
@@ -454,15 +472,11 @@ CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st,
     VisitCount vc;
     const bool found = intersect<false, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
                                                h, err, &vc);
-    st.hit_tri[path] = found ? h.tri : kNoTriangle;
-    if (st.guide.hitT) st.guide.hitT[path] = found ? static_cast<float>(h.t) : 0.0f;
-    if (err) raise(E, P, st.pixel[path], st.sample[path], err);
     if (COUNT) {
         atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
         atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
     }
-    if (!found) return kShadeMiss;
-    return (S.nee_skip && (h.flags & kTriNeeNull)) ? kShadeNeeNull : kShadeGeneric;
+    return closestFinish(S, P, st, path, E, found, h, err);
 }
 
 // The job of a path in the multi-job pool.

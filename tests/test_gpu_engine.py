@@ -109,6 +109,44 @@ def test_batch_solo_jobs(crgpu, world):
     assert failing.status == e.value.status and failing.error == str(e.value)
 
 
+def _foliage(crgpu):
+    """An alpha-cutout textured quad under a directional light (test_integrator.cpp's foliage
+    fixture): a scene that needs the full kernels (alpha test, texture lookups, punctual light)."""
+    from crgpu import ALPHA_MASK, WRAP_REPEAT, new_materials, texture_dtype
+    m = new_materials(2)
+    m[0]["metallic"] = 0; m[0]["base_color"][:3] = (0.4, 0.35, 0.25)
+    m[1]["metallic"] = 0; m[1]["double_sided"] = 1; m[1]["alpha_mode"] = ALPHA_MASK
+    m[1]["base_color"][:3] = (0.12, 0.45, 0.04)
+    images = [np.array([[[1, 1, 1, 1], [1, 1, 1, 0]], [[1, 1, 1, 0], [1, 1, 1, 1]]], np.float32)]
+    textures = np.zeros(1, texture_dtype)
+    textures[0] = (0, WRAP_REPEAT, WRAP_REPEAT, 0)
+    m[1]["base_color_texture"]["texture"] = 0
+    tris = scenes.cat(scenes.quad((-8, -0.8, 8), (8, -0.8, 8), (8, -0.8, -8), (-8, -0.8, -8), 0),
+                      scenes.quad((-0.8, -0.7, 0), (0.8, -0.7, 0), (0.8, 0.9, 0), (-0.8, 0.9, 0), 1))
+    sc = dict(triangles=tris, materials=m, images=images, textures=textures,
+              lights=scenes.directional(scenes.normalize((-1, -2, -1)), 2))
+    return gpu_scene(crgpu, sc, env=crgpu.env_desc(constant=(0.3, 0.3, 0.3)))
+
+
+def test_batch_mixing_full_and_lean_scenes(crgpu, world):
+    """While a job whose scene has textures, alpha masks and a punctual light is in the pool,
+    the steps run the full kernels; once it has ended, the lean ones. Every film is its
+    standalone render's either way."""
+    foliage = _foliage(crgpu)
+    try:
+        jobs = [JobSpec(foliage, scenes.room_camera(), _opts(crgpu, 32, 32, 8, bounces=8)),
+                JobSpec(world["room"], world["room_cam"], _opts(crgpu, 64, 48, 16)),
+                JobSpec(world["grid"], world["grid_cam"], _opts(crgpu, 96, 54, 8, seed=5))]
+        stats = render_batch(jobs, EngineTuning.make(pool_paths=4096, range_samples=2048, solo_samples_log2=64))
+        assert stats["jobs_done"] == 3
+        for i, j in enumerate(jobs):
+            assert j.status == 0, j.error
+            film, _ = _alone(j)
+            assert np.array_equal(j.film, film), f"job {i}"
+    finally:
+        foliage.close()
+
+
 def test_batch_progressive_frames(crgpu, world):
     jobs = [JobSpec(world["room"], world["room_cam"], _opts(crgpu, 40, 30, 10), every=4, fmt=0, exposure=0.5),
             JobSpec(world["grid"], world["grid_cam"], _opts(crgpu, 64, 36, 6, seed=3), every=2, fmt=2),

@@ -484,17 +484,16 @@ void build_alias(EnvTables& out) {
     }
 }
 
-void build_lights(const cr_triangle* triangles, uint64_t count, const cr_material* materials,
-                  const cr_punctual_light* lights, uint32_t lightCount, double envIntegral, LightTables& out) {
-    out = LightTables{};
-    out.triangleProbability.assign(count, 0.0f);
+LightScan scan_lights(const cr_triangle* triangles, uint64_t count, const cr_material* materials) {
     // The scene box and the emitters' weights in parallel: positions are finite after
     // finalize, so min/max in any order give the same box; the weights go into per-part lists
-    // that are then read in triangle order, so the running total below is summed in the
+    // that build_lights reads in triangle order, so its running total is summed in the
     // reference's order.
     constexpr uint64_t kParts = 64;
+    LightScan scan;
+    scan.count = count;
     std::vector<Bounds> partBox(kParts);
-    std::vector<std::vector<std::pair<uint32_t, double>>> partEmitters(kParts);
+    scan.emitters.resize(kParts);
     parallel_for(kParts, [&](uint64_t pb, uint64_t pe) {
         for (uint64_t part = pb; part < pe; ++part) {
             const uint64_t b = count * part / kParts, e = count * (part + 1) / kParts;
@@ -504,14 +503,27 @@ void build_lights(const cr_triangle* triangles, uint64_t count, const cr_materia
                 local.expand(triangleBounds(t));
                 const cr_material& m = materials[t.material];
                 const double w = static_cast<double>(t.area) * pi * luminance(v3(m.emission)) * (m.double_sided ? 2 : 1);
-                if (w > 0) partEmitters[part].push_back({static_cast<uint32_t>(i), w});
+                if (w > 0) scan.emitters[part].push_back({static_cast<uint32_t>(i), w});
             }
             partBox[part] = local;
         }
     }, 1);
     Bounds box;
     for (const Bounds& b : partBox) box.expand(b);
-    const double radius2 = count == 0 ? 1 : std::max(1.0, static_cast<double>(lengthSquared(box.hi - box.lo)) * 0.25);
+    scan.radius2 = count == 0 ? 1 : std::max(1.0, static_cast<double>(lengthSquared(box.hi - box.lo)) * 0.25);
+    return scan;
+}
+
+void build_lights(const cr_triangle* triangles, uint64_t count, const cr_material* materials,
+                  const cr_punctual_light* lights, uint32_t lightCount, double envIntegral, LightTables& out) {
+    build_lights(scan_lights(triangles, count, materials), lights, lightCount, envIntegral, out);
+}
+
+void build_lights(const LightScan& scan, const cr_punctual_light* lights, uint32_t lightCount, double envIntegral,
+                  LightTables& out) {
+    out = LightTables{};
+    out.triangleProbability.assign(scan.count, 0.0f);
+    const double radius2 = scan.radius2;
     double total = 0;
     auto add = [&](uint32_t type, uint32_t index, double weight) {
         if (weight > 0) { total += weight; out.entries.push_back({total, type, index, 0.0f, 0u}); }
@@ -521,7 +533,7 @@ void build_lights(const cr_triangle* triangles, uint64_t count, const cr_materia
         add(crg::kLightPunctual, i, static_cast<double>(luminance(v3(l.color))) * l.intensity *
                                         (l.type == CR_LIGHT_DIRECTIONAL ? pi * radius2 : 4 * pi));
     }
-    for (const auto& part : partEmitters)
+    for (const auto& part : scan.emitters)
         for (const auto& [index, weight] : part) add(crg::kLightTriangle, index, weight);
     add(crg::kLightEnvironment, 0, envIntegral * pi * radius2);
     double last = 0, cumulative = 0;

@@ -5,6 +5,7 @@
 #include <stdexcept>
 #include <string>
 #include <functional>
+#include <utility>
 #include <vector>
 #include "cr_gpu.h"
 #include "cr_internal.h"
@@ -57,6 +58,17 @@ struct LightTables {
     std::vector<float> triangleProbability;
     float environmentProbability = 0;
 };
+// The triangle half of the light table (the scene's bounding radius and the emitters' weights,
+// per part in triangle order), which needs no environment: a scene upload computes it while
+// the environment tables are still being built.
+struct LightScan {
+    uint64_t count = 0;
+    double radius2 = 1;
+    std::vector<std::vector<std::pair<uint32_t, double>>> emitters;
+};
+LightScan scan_lights(const cr_triangle* triangles, uint64_t count, const cr_material* materials);
+void build_lights(const LightScan& scan, const cr_punctual_light* lights, uint32_t lightCount, double envIntegral,
+                  LightTables& out);
 void build_lights(const cr_triangle* triangles, uint64_t count, const cr_material* materials,
                   const cr_punctual_light* lights, uint32_t lightCount, double envIntegral, LightTables& out);
 

@@ -183,6 +183,50 @@ class Staging {
     std::unique_ptr<unsigned char[]> fallback_;
 };
 
+// Copies host memory (the caller's, pageable) to the device through page-locked chunks: a few
+// host threads fill one chunk while the chunks before it are in transfer, so the copy runs near
+// the host's memcpy rate rather than the driver's pageable path (~9 GB/s measured). Returns when
+// the copy is complete.
+void stagedUpload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    constexpr size_t kChunk = size_t{16} << 20;
+    constexpr int kRing = 3;
+    if (bytes < kChunk) {
+        CR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    auto [block, have] = PinnedCache::get().take(kRing * kChunk);
+    if (!block) {  // no page-locked memory to be had: the driver's own path
+        CR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        CR_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    struct Ring {
+        void* block;
+        size_t size;
+        cudaStream_t s;
+        cudaEvent_t done[kRing] = {};
+        ~Ring() {
+            cudaStreamSynchronize(s);
+            for (cudaEvent_t e : done) if (e) cudaEventDestroy(e);
+            PinnedCache::get().give(block, size);
+        }
+    } ring{block, have, s};
+    for (auto& e : ring.done) CR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    unsigned char* const base = static_cast<unsigned char*>(block);
+    const unsigned char* const from = static_cast<const unsigned char*>(src);
+    for (size_t off = 0, i = 0; off < bytes; off += kChunk, ++i) {
+        const size_t len = std::min(kChunk, bytes - off);
+        const int k = static_cast<int>(i % kRing);
+        unsigned char* const buf = base + k * kChunk;
+        if (i >= kRing) CR_CUDA(cudaEventSynchronize(ring.done[k]));  // the slot's last transfer is done
+        crh::parallel_for(len, [&](uint64_t b, uint64_t e) { std::memcpy(buf + b, from + off + b, e - b); }, size_t{4} << 20);
+        CR_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, buf, len, cudaMemcpyHostToDevice, s));
+        CR_CUDA(cudaEventRecord(ring.done[k], s));
+    }
+    CR_CUDA(cudaStreamSynchronize(s));
+}
+
 // Parts of a scene upload that run on host threads beside the caller's: task k runs on its
 // own thread with the scene's device current and copies on stream(k); join(k) waits for the
 // task and its copies and rethrows its exception. The destructor joins whatever is left.
@@ -279,16 +323,22 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     SideWork side(g.device);
     S.tris = g.geometry.alloc<cr_triangle>(n);
     side.run(0, [&, dst = const_cast<cr_triangle*>(S.tris)] {
-        if (n) CR_CUDA(cudaMemcpyAsync(dst, d.triangles, n * sizeof(cr_triangle), cudaMemcpyHostToDevice, side.stream(0)));
+        if (n) stagedUpload(dst, d.triangles, n * sizeof(cr_triangle), side.stream(0));
     });
     side.run(1, [&] {
         crh::build_environment(env, E);
         if (E.hasImage) {
             const cudaStream_t es = side.stream(1);
             const size_t px = static_cast<size_t>(E.width) * E.height;
-            S.env_pixels = envMem.upload(reinterpret_cast<const float4*>(env.pixels), px, es);
-            S.env_cdf = envMem.upload(E.cdf.data(), E.cdf.size(), es);
-            S.env_pdf = envMem.upload(E.pdf.data(), E.pdf.size(), es);
+            float4* pixels = envMem.alloc<float4>(px);
+            stagedUpload(pixels, env.pixels, px * sizeof(float4), es);
+            S.env_pixels = pixels;
+            double* cdf = envMem.alloc<double>(E.cdf.size());
+            stagedUpload(cdf, E.cdf.data(), E.cdf.size() * sizeof(double), es);
+            S.env_cdf = cdf;
+            float* pdf = envMem.alloc<float>(E.pdf.size());
+            stagedUpload(pdf, E.pdf.data(), E.pdf.size() * sizeof(float), es);
+            S.env_pdf = pdf;
             S.env_row_cos = envMem.upload(E.rowCos.data(), E.rowCos.size(), es);
             S.env_coarse = envMem.upload(E.coarse.data(), E.coarse.size(), es);
         }
@@ -427,6 +477,8 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     NodePair* devPairs = g.geometry.alloc<NodePair>(pairSlots);
     CR_CUDA(cudaMemcpyAsync(devPairs, pairs, pairSlots * sizeof(NodePair), cudaMemcpyHostToDevice, s));
     S.pairs = devPairs;
+    // the triangle half of the light table, while the helpers finish
+    const crh::LightScan lightScan = crh::scan_lights(d.triangles, n, d.materials);
     side.join(0);  // the triangle records
     S.any_alpha_mask = anyMask;
     // A textured emitter's light sample evaluates textures, which can fail; keep it then.
@@ -470,7 +522,7 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     S.env_intensity = E.intensity;
     // lights
     crh::LightTables L;
-    crh::build_lights(d.triangles, n, d.materials, d.lights, d.light_count, E.integral, L);
+    crh::build_lights(lightScan, d.lights, d.light_count, E.integral, L);
     S.light_entries = g.geometry.upload(L.entries.data(), L.entries.size(), s);
     S.light_entry_count = static_cast<uint32_t>(L.entries.size());
     S.tri_light_probability = g.geometry.upload(L.triangleProbability.data(), L.triangleProbability.size(), s);

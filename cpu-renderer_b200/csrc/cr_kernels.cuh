@@ -13,12 +13,6 @@
 #ifndef CR_TRACE_MIN_BLOCKS
 #define CR_TRACE_MIN_BLOCKS 12
 #endif
-#ifndef CR_DYNAMIC_TRACE
-#define CR_DYNAMIC_TRACE 1
-#endif
-#ifndef CR_DYNAMIC_SHADE
-#define CR_DYNAMIC_SHADE 1
-#endif
 #ifndef CR_SHADE_MIN_BLOCKS
 #define CR_SHADE_MIN_BLOCKS 4
 #endif
@@ -613,14 +607,9 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
         stats[kStatShadowRays] += nS;
     }
     const uint32_t total = nE + nS;
-#if CR_DYNAMIC_TRACE
     for (uint32_t base = warpTake(&q.counts[kCountTraceWork0 + cur]); base < total;
          base = warpTake(&q.counts[kCountTraceWork0 + cur])) {
         const uint32_t idx = base + (threadIdx.x & 31);
-#else
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-#endif
         bool freed = false;
         int cls = -1;
         uint32_t path = 0, r = 0;
@@ -656,14 +645,9 @@ __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                                                unsigned long long* stats, JobTable J) {
     const uint32_t n = q.counts[kCountShade0 + CLASS];
     const uint32_t* in = q.shade[CLASS];
-#if CR_DYNAMIC_SHADE
     for (uint32_t base = warpTake(&q.counts[kCountShadeWork0 + CLASS]); base < n;
          base = warpTake(&q.counts[kCountShadeWork0 + CLASS])) {
         const uint32_t idx = base + (threadIdx.x & 31);
-#else
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t idx = base + threadIdx.x;
-#endif
         bool cont = false, shadow = false, freed = false;
         uint32_t path = 0, r = 0;
         if (idx < n) {

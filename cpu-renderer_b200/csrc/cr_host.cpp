@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <numeric>
 #include <sstream>
 #include <thread>
@@ -413,7 +414,7 @@ void build_environment(const cr_environment_desc& e, EnvTables& out, bool alias)
     for (int y = 0; y < H; ++y) omegas[y] = solidAngle(y);
     // Texel weights in parallel; the running sums below stay sequential, in the reference's
     // order, so the CDF is bit-identical (render.cpp:29-41).
-    std::vector<double> light(n);
+    std::unique_ptr<double[]> light(new double[n]);  // every entry is written below
     std::atomic<bool> bad{false};
     parallel_for(n, [&](uint64_t b, uint64_t en) {
         for (uint64_t i = b; i < en; ++i) {
@@ -424,7 +425,7 @@ void build_environment(const cr_environment_desc& e, EnvTables& out, bool alias)
         }
     });
     if (bad) throw Error(CR_ERR_INVALID_ARGUMENT, "Non-finite or negative HDR environment pixel");
-    out.cdf.resize(n);
+    out.cdf.reserve(n);  // appended in order, without a zero fill first
     for (int y = 0; y < H; ++y) {
         const double omega = omegas[y];
         const size_t row = static_cast<size_t>(y) * W;
@@ -432,7 +433,7 @@ void build_environment(const cr_environment_desc& e, EnvTables& out, bool alias)
             const double l = light[row + x];
             out.integral += l * omega;
             out.weightSum += (l + 1e-9) * omega;
-            out.cdf[row + x] = out.weightSum;
+            out.cdf.push_back(out.weightSum);
         }
     }
     if (e.cdf) {  // the caller's own copy of the same table

@@ -11,13 +11,17 @@
 //             the job with the fewest samples per pixel issued, while the per-sample
 //             radiance arena has room and the pool is not already fed a pool's worth ahead
 //   run       iterations_per_step iterations of k_regen / k_trace / k_shade x3 (one CUDA
-//             graph when use_graphs), k_regen refilling freed slots every refill_interval
+//             graph per kernel variant when use_graphs), k_regen refilling freed slots every
+//             refill_interval; the variant drops the alpha test and the texture and punctual
+//             light code when no active job's scene needs them
 //   complete  finished-sample counters are read back; a job's ranges are summed into its
 //             pixel sums strictly in order (k_accumulate), so the film is the ordered FP64
 //             sum of its samples exactly as in a single render; frames and results go out
 //
 // A job whose sample fails stops taking new ranges; once its issued ranges have drained, the
 // failing sample is re-run alone to recover the reference's message, as a single render does.
+// In a batch, jobs that fill the pool on their own render alone through the single-render
+// entry points, on a helper thread beside the pool (runBatch).
 #include "cr_kernels.cuh"
 #include "cr_driver.h"
 #include "cr_encode.h"

@@ -1,17 +1,19 @@
 // Wavefront path tracer for sm_100a: kernels and the host driver behind include/cr_gpu.h.
 //
 // One render (cr::render, render.cpp:352-456) runs a pool of path slots. Camera samples are
-// numbered sample-major (id = sample * pixels + pixel) and issued in order to free slots.
-// Every iteration runs three launches over the whole pool:
+// numbered sample-major (id = sample * pixels + pixel) and issued in order to free slots, a
+// chunk of ids at a time (by default one pool's worth: every slot starts a sample at the
+// chunk's first iteration and the chunk drains). Every iteration runs these launches:
 //
 //   k_regen   free slots take the next sample ids: jitter + camera ray   (render.cpp:396-401)
 //   k_trace   closest hit for the live queue (Bvh::intersect, geometry.cpp:554) and any hit for
 //             the shadow rays queued by the previous iteration, in one launch
-//   k_shade   one trace() iteration per live path (render.cpp:240-344)
-//             -> next live queue, shadow queue, free queue (warp-ballot compaction)
+//   k_shade   one trace() iteration per live path (render.cpp:240-344), one launch per
+//             material class -> next live queue, shadow queue, free queue (warp ballots)
 //
-// Finished paths are refilled the next iteration, so launches stay full until the last
-// samples drain. Each path keeps the reference's order of random draws and radiance sums, so a
+// Warps take 32-entry batches of a queue from a counter, so a launch ends when its work does.
+// Scenes without alpha masks, textures or punctual lights run instantiations compiled without
+// that code. Each path keeps the reference's order of random draws and radiance sums, so a
 // camera sample consumes the same SplitMix stream as on the CPU. Every sample's radiance is
 // stored by id; at the end of a chunk of ids, k_accumulate adds each pixel's samples in index
 // order into FP64 sums (render.cpp:388-415), so the film does not depend on scheduling.

@@ -137,13 +137,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per traced ray (closest or any hit) of k_trace from the committed ncu summary."""
+def profile_summary():
+    """The committed ncu summary of k_trace (DRAM bytes per traced ray, L2 throughput), or {}."""
     path = os.path.join(ROOT, "profiles", "k_trace_sphere_grid.json")
     if not os.path.exists(path):
-        return None
+        return {}
     with open(path) as f:
-        return json.load(f).get("dram_bytes_per_traced_ray")
+        return json.load(f)
+
+
+def profile_traffic():
+    """DRAM bytes per traced ray (closest or any hit) of k_trace from the committed ncu summary."""
+    return profile_summary().get("dram_bytes_per_traced_ray")
 
 
 def cpu_reference_rate(sc, spp, threads):
@@ -257,6 +262,7 @@ def run_ours(args):
         "kernel": "k_trace (closest + any hit)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": peak_kind,
         "traffic": (traffic_per_ray * rays / trace_launches) if traffic_per_ray else None,
+        "l2": profile_summary().get("l2"),
         "algorithmic_bytes_per_launch": algo_bytes / trace_launches,
         "closest_hit": {"bytes_per_ray": ext_bytes, "pairs_per_ray": ext_pairs, "triangles_per_ray": ext_tris},
         "any_hit": {"bytes_per_ray": sh_bytes, "pairs_per_ray": sh_pairs, "triangles_per_ray": sh_tris},

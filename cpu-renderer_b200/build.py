@@ -87,6 +87,9 @@ def build(force=False, verbose=False, ptxas_verbose=False, defines=(), out=None)
     tmp = lib + ".tmp"
     _run([nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", tmp] + dev_objs + [host_obj, "-lpthread"], verbose)
     os.replace(tmp, lib)
+    if tag:  # a variant build's objects are not reused: do not let them pile up in _build
+        for obj in dev_objs:
+            os.remove(obj)
     return lib
 
 

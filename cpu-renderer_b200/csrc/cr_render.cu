@@ -94,6 +94,18 @@ struct Workspace {
     int gridTrace = 0, gridShade = 0, gridShadeLight = 0, gridShadeMiss = 0, gridRegen = 0, gridSmall = 0;
     int gridShadeLean = 0, gridShadeLightLean = 0, gridShadeMissLean = 0, gridTraceNoAlpha = 0;
     std::vector<cudaEvent_t> events;
+    // two more streams for the shading launches that run beside the generic one
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+
+    void ensureSideStreams() {
+        if (side[0]) return;
+        CR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        for (int k = 0; k < 2; ++k) {
+            CR_CUDA(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+            CR_CUDA(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming));
+        }
+    }
 
     cudaEvent_t event(size_t i) {
         while (events.size() <= i) {
@@ -617,6 +629,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     Workspace& W = workspaceFor(g.device);
     std::lock_guard<std::mutex> wsLock(W.mutex);
     W.ensureWork(static_cast<size_t>(pool));
+    W.ensureSideStreams();
     W.ensureOut(static_cast<size_t>(chunk));
     g.ensureFilm(pixels);
     if (perSample) W.ensurePacked(static_cast<size_t>(chunk));
@@ -739,7 +752,28 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     else if (noAlpha) k_trace<false, false, true><<<cap(W.gridTraceNoAlpha), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                     else k_trace<false><<<cap(W.gridTrace), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                 });
-                // shading: the lean instantiations when the scene allows them
+                // shading: the lean instantiations when the scene allows them. The classes'
+                // queues are independent, so without phase timing or guiding the miss and
+                // NEE-null launches run on two more streams beside the generic one, and each
+                // fills the device while the others drain.
+                if (!timePhases && !guide) {
+                    CR_CUDA(cudaEventRecord(W.fork, s));
+                    for (int k = 0; k < 2; ++k) CR_CUDA(cudaStreamWaitEvent(W.side[k], W.fork, 0));
+                    if (lean) {
+                        k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, W.side[0]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, W.side[1]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    } else {
+                        k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, W.side[0]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, W.side[1]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    }
+                    for (int k = 0; k < 2; ++k) {
+                        CR_CUDA(cudaEventRecord(W.join[k], W.side[k]));
+                        CR_CUDA(cudaStreamWaitEvent(s, W.join[k], 0));
+                    }
+                    launches += 3;
+                } else {
                 if (lean) {
                     rec(1, [&] { k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                     rec(1, [&] { k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
@@ -760,6 +794,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     rec(1, [&] { k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else {
                     rec(1, [&] { k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                }
                 }
                 cur ^= 1;
                 ++iter;

@@ -120,10 +120,10 @@ CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     }
     st.ray_o[slot] = f4(ray.o, ray.tmin);
     st.ray_d[slot] = f4(ray.d, ray.tmax);
-    st.ray_lo[slot] = make_float4(0, 0, 0, 0);
+    if (precise) st.ray_lo[slot] = make_float4(0, 0, 0, 0);  // read only for precise rays
     st.thr[slot] = make_float4(1, 1, 1, 1);          // throughput 1, etaScale 1
     st.rad[slot] = make_float4(0, 0, 0, 0);          // radiance 0, lastPdf 0
-    st.last_pos[slot] = make_float4(0, 0, 0, 0);
+    // last_pos needs no value yet: it is read only after a non-delta bounce, which writes it
     st.absorb[slot] = make_float4(0, 0, 0, __int_as_float(-1));  // medium -1
     st.flags[slot] = kPathLastDelta | (precise ? kPathPrecise : 0u);
     st.rng[slot] = rng.state;

@@ -159,8 +159,8 @@ def cpu_reference_rate(sc, spp, threads):
     rs = refimpl.RefScene(sc["triangles"], sc["materials"]).build_bvh()
     env = refimpl.RefEnvironment(image=sc["env_image"])
     o = sc["options"]
-    import crgpu
-    opt = crgpu.Options.make(width=o.width, height=o.height, samples=spp, bounces=o.bounces, threads=threads, seed=o.seed)
+    from cr_types import Options
+    opt = Options.make(width=o.width, height=o.height, samples=spp, bounces=o.bounces, threads=threads, seed=o.seed)
     film, st = rs.render(sc["camera"], opt, env)
     return st["camera_samples"] / st["seconds"] / 1e6, st
 
@@ -174,13 +174,16 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libcr_ref.so was not built"}))
         return
     threads = os.cpu_count() or 1
-    sc, _, _, _ = build_workload(args.spp)
+    # the scene generator and the ctypes layouts only: the reference finalizes the scene and
+    # builds its BVH itself, and the product library is never loaded on this arm
+    import workloads
+    from cr_types import Options
+    sc = workloads.sphere_grid_scene(samples=args.spp)
     rs = refimpl.RefScene(sc["triangles"], sc["materials"]).build_bvh()
     env = refimpl.RefEnvironment(image=sc["env_image"])
-    import crgpu
     o = sc["options"]
     step_spp = 1  # one step: the full 1920x1080 frame at 1 spp of the same streams
-    opt = crgpu.Options.make(width=o.width, height=o.height, samples=step_spp, bounces=o.bounces, threads=threads, seed=o.seed)
+    opt = Options.make(width=o.width, height=o.height, samples=step_spp, bounces=o.bounces, threads=threads, seed=o.seed)
     for _ in range(args.warmup):
         rs.render(sc["camera"], opt, env)
     secs = []
@@ -194,7 +197,9 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded procedural scene and sky)",
         "config": {"workload": WORKLOAD, "triangles": 1 << 20, "width": o.width, "height": o.height, "spp": args.spp,
-                   "bounces": o.bounces, "step": f"{o.width}x{o.height} x {step_spp} spp of the same sample streams"},
+                   "bounces": o.bounces, "step": f"{o.width}x{o.height} x {step_spp} spp of the same sample streams",
+                   "same_config": "same scene, frame, bounces and per-sample streams; a step is 1 of the 64 samples "
+                                  "per pixel, so the per-sample rate is comparable and the step is 1/64 of the render"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{o.width}x{o.height} x {step_spp} spp per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -242,6 +247,21 @@ def run_ours(args):
             launches += st["kernel_launches"]
     max_ms = ranks.max_over_ranks(sum(dev_ms))
     value = ranks.whole_job_rate(samples_per_step * args.steps, max_ms / 1e3)
+
+    # the same renders with alias-table environment sampling (other sample streams, the same
+    # unbiased estimator): K more timed steps after one untimed render that builds the table
+    ta = crgpu.Tuning()
+    ta.env_alias = 1
+    g.render_resident(cam, opt, tuning=ta)
+    alias_ms = []
+    for _ in range(args.steps):
+        flush_l2(torch, device)
+        barrier()
+        st, _ = g.render_resident(cam, opt, tuning=ta)
+        barrier()
+        alias_ms.append(st["device_ms"])
+    alias_max = ranks.max_over_ranks(sum(alias_ms))
+    alias_value = ranks.whole_job_rate(samples_per_step * args.steps, alias_max / 1e3)
 
     # dominant-kernel timing: one more render with CUDA events around every launch
     tp = crgpu.Tuning()
@@ -314,6 +334,10 @@ def run_ours(args):
                     "step_seconds": [round(x, 4) for x in e2e_secs],
                     "note": "cr_gpu_scene_create (upload) + cr_gpu_render (film download) + destroy from host arrays, "
                             "every one of K steps, after one untimed step of the same kind"},
+            "env_alias": {"value": alias_value, "unit": UNIT, "ms_per_step": alias_max / args.steps,
+                          "note": "alias-table environment sampling instead of the reference's CDF search "
+                                  "(different sample streams, exact realised texel densities); value above is "
+                                  "the CDF (reference-stream) mode"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
         }

@@ -94,6 +94,7 @@ class PinnedCache {
             }
         }
         void* p = nullptr;
+        crh::count_allocation();
         if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
             cudaGetLastError();
             return {nullptr, 0};
@@ -127,6 +128,7 @@ struct DevAlloc {
         const size_t want = count * sizeof(T);
         int device = 0;
         CR_CUDA(cudaGetDevice(&device));
+        crh::count_allocation();
         auto [p, have] = BlockCache::get().take(device, want);
         if (!p) {
             if (cudaMalloc(&p, want) != cudaSuccess) {
@@ -199,6 +201,7 @@ struct cr_gpu_scene {
     uint64_t triangleCount = 0;
     crh::EnvTables env;  // host copy, for the alias table built on demand
     crd::DevAlloc aliasAlloc;
+    const float* aliasPdf = nullptr;  // the alias sampler's texel densities (device), once built
     // film of the last render: FP64 sums and the float film
     double* acc = nullptr;
     float* film = nullptr;

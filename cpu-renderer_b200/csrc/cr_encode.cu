@@ -205,6 +205,7 @@ void grow(T*& p, uint64_t& cap, uint64_t need) {
     if (p) ENC_CUDA(cudaFree(p));
     p = nullptr;
     cap = 0;
+    crh::count_allocation();
     if (cudaMalloc(&p, need * sizeof(T)) != cudaSuccess) {
         cudaGetLastError();
         throw crh::Error(CR_ERR_OUT_OF_MEMORY, "device allocation for output encoding failed");
@@ -234,6 +235,7 @@ uint64_t encode_film(const float* dFilm, int width, int height, int format, floa
     EncodeCache& E = cacheFor(device);
     std::lock_guard<std::mutex> lock(E.encodeMutex);
     if (!E.check) {
+        for (int k = 0; k < 3; ++k) crh::count_allocation();
         ENC_CUDA(cudaMalloc(&E.check, sizeof(Check)));
         ENC_CUDA(cudaMalloc(&E.thresholds, 256 * sizeof(float)));
         ENC_CUDA(cudaMallocHost(&E.hostCheck, sizeof(Check)));

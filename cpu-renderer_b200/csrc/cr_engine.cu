@@ -150,6 +150,7 @@ class Engine {
         one_.out = scratchAlloc_.alloc<float4>(1);
         oneDetail_ = scratchAlloc_.alloc<DevError>(1);
         oneStats_ = scratchAlloc_.alloc<unsigned long long>(2);
+        for (int k = 0; k < 6; ++k) crh::count_allocation();
         CR_CUDA(cudaMallocHost(&hRanges_, kMaxRanges * sizeof(IssueRange)));
         CR_CUDA(cudaMallocHost(&hDone_, kMaxRanges * sizeof(unsigned long long)));
         CR_CUDA(cudaMallocHost(&hCtl_, 4 * sizeof(unsigned long long)));

@@ -241,6 +241,12 @@ cr_status set_last_error(cr_status status, const std::string& message) {
     return status;
 }
 
+namespace {
+std::atomic<uint64_t> g_allocations{0};
+}
+void count_allocation() { g_allocations.fetch_add(1, std::memory_order_relaxed); }
+uint64_t allocation_count() { return g_allocations.load(std::memory_order_relaxed); }
+
 void validate_options(const cr_render_options& o) {
     if (o.width < 1 || o.height < 1 || o.width > 16384 || o.height > 16384)
         throw Error(CR_ERR_INVALID_ARGUMENT, "Width and height must be in [1, 16384]");
@@ -463,14 +469,51 @@ void build_environment(const cr_environment_desc& e, EnvTables& out, bool alias)
     if (alias) build_alias(out);
 }
 
+// Walker's alias method (Walker 1977) with Vose's construction (Vose 1991) over the texel
+// probabilities of the CDF. The device draws a 48-bit uniform x (two 24-bit draws) and forms
+// x*n = col*2^48 + r: col is the column, r the residual. The x of column c are the integers
+// x0_c, x0_c+1, ... (count_c of them, x0_c = ceil(c*2^48/n)) and their residuals rise in steps
+// of n from r0_c = x0_c*n - c*2^48, so "the first K_c of them take texel c, the rest its alias"
+// is the test r < K_c*n + r0_c. With K_c = round(threshold_c * count_c) every texel's
+// probability under the sampler is an exact integer count over 2^48; the density the sampler
+// reports, for light samples and for the MIS weight of BSDF-sampled directions alike, is that
+// probability over the texel's solid angle, so the estimator is unbiased however the
+// thresholds rounded.
+namespace {
+constexpr int kAliasBits = 48;
+struct AliasColumn {
+    uint64_t count, r0;
+};
+AliasColumn alias_column(uint64_t c, uint64_t n) {
+    using u128 = unsigned __int128;
+    auto ceilDiv = [&](u128 a) { return static_cast<uint64_t>((a + n - 1) / n); };
+    const u128 lo = static_cast<u128>(c) << kAliasBits, hi = static_cast<u128>(c + 1) << kAliasBits;
+    const uint64_t x0 = ceilDiv(lo), x1 = ceilDiv(hi);
+    return {x1 - x0, static_cast<uint64_t>(static_cast<u128>(x0) * n - lo)};
+}
+}  // namespace
+
+std::vector<uint64_t> alias_masses(const EnvTables& t) {
+    const uint64_t n = t.aliasThreshold.size();
+    std::vector<uint64_t> mass(n, 0);
+    for (uint64_t c = 0; c < n; ++c) {
+        const AliasColumn col = alias_column(c, n);
+        // K_c: how many of the column's x fall below its threshold
+        const uint64_t T = t.aliasThreshold[c];
+        const uint64_t own = T <= col.r0 ? 0 : std::min<uint64_t>(col.count, (T - col.r0 + n - 1) / n);
+        mass[c] += own;
+        mass[t.aliasIndex[c]] += col.count - own;
+    }
+    return mass;
+}
+
 void build_alias(EnvTables& out) {
-    if (!out.hasImage || !out.aliasProb.empty()) return;
-    const size_t n = out.cdf.size();
-    out.aliasProb.assign(n, 1.0f);
+    if (!out.hasImage || !out.aliasThreshold.empty()) return;
+    const uint64_t n = out.cdf.size();
+    std::vector<double> threshold(n, 1.0), scaled(n);
     out.aliasIndex.resize(n);
-    std::vector<double> scaled(n);
     std::vector<uint32_t> small, large;
-    for (size_t i = 0; i < n; ++i) {
+    for (uint64_t i = 0; i < n; ++i) {
         scaled[i] = (out.cdf[i] - (i ? out.cdf[i - 1] : 0)) / out.weightSum * static_cast<double>(n);
         out.aliasIndex[i] = static_cast<uint32_t>(i);
         (scaled[i] < 1.0 ? small : large).push_back(static_cast<uint32_t>(i));
@@ -478,10 +521,27 @@ void build_alias(EnvTables& out) {
     while (!small.empty() && !large.empty()) {
         const uint32_t sm = small.back(); small.pop_back();
         const uint32_t l = large.back();
-        out.aliasProb[sm] = static_cast<float>(scaled[sm]);
+        threshold[sm] = scaled[sm];
         out.aliasIndex[sm] = l;
         scaled[l] = (scaled[l] + scaled[sm]) - 1.0;
         if (scaled[l] < 1.0) { large.pop_back(); small.push_back(l); }
+    }
+    // columns left on either list keep threshold 1 (rounding leftovers: their own texel)
+    out.aliasThreshold.resize(n);
+    for (uint64_t c = 0; c < n; ++c) {
+        const AliasColumn col = alias_column(c, n);
+        const double k = std::nearbyint(std::min(1.0, std::max(0.0, threshold[c])) * static_cast<double>(col.count));
+        const uint64_t K = std::min<uint64_t>(col.count, static_cast<uint64_t>(k));
+        out.aliasThreshold[c] = K * n + col.r0;
+    }
+    const std::vector<uint64_t> mass = alias_masses(out);
+    out.aliasPdf.resize(n);
+    const int W = out.width, H = out.height;
+    for (uint64_t i = 0; i < n; ++i) {
+        const int y = static_cast<int>(i / static_cast<uint64_t>(W));
+        const double a = static_cast<double>(pi) * y / H, b = static_cast<double>(pi) * (y + 1) / H;
+        const double omega = (2 * static_cast<double>(pi) / W) * (std::cos(a) - std::cos(b));
+        out.aliasPdf[i] = static_cast<float>(std::ldexp(static_cast<double>(mass[i]), -kAliasBits) / omega);
     }
 }
 

@@ -20,6 +20,11 @@ struct Error : std::runtime_error {
 
 cr_status set_last_error(cr_status status, const std::string& message);
 
+// Memory blocks the library has requested (device and page-locked host): every allocation
+// site calls count_allocation(); cr_gpu_allocation_count reports the total.
+void count_allocation();
+uint64_t allocation_count();
+
 void validate_options(const cr_render_options& o);                           // render.cpp:97-104
 
 // Scene::finalize (geometry.cpp:296-397) on a triangle vector.
@@ -42,12 +47,18 @@ struct EnvTables {
     std::vector<float> pdf;       // per texel density
     std::vector<float> rowCos;    // cos(pi*y/H) for y = 0..H
     std::vector<uint32_t> coarse; // bracket table for the CDF search
-    std::vector<float> aliasProb;
+    // alias-table sampling (built on demand): per column the threshold on the 48-bit residual
+    // below which the column's own texel is taken, its alias, and every texel's density under
+    // this sampler (its realised probability, exact, over the texel's solid angle)
+    std::vector<uint64_t> aliasThreshold;
     std::vector<uint32_t> aliasIndex;
+    std::vector<float> aliasPdf;
 };
 void build_environment(const cr_environment_desc& e, EnvTables& out, bool alias = false);
 // Walker/Vose alias table over the same texel probabilities (built on demand).
 void build_alias(EnvTables& t);
+// The alias sampler's realised probability of every texel, in units of 2^-48 (for checks).
+std::vector<uint64_t> alias_masses(const EnvTables& t);
 
 // Runs fn(begin, end) over [0, n) split across the host's hardware threads.
 void parallel_for(uint64_t n, const std::function<void(uint64_t, uint64_t)>& fn, uint64_t grain = 65536);

@@ -84,8 +84,10 @@ struct DevScene {
     uint32_t env_coarse_count;    // entries in env_coarse (a power of two)
     double env_weight_sum;
     float env_rotation, env_intensity;
-    const float* alias_prob;      // alias-table sampling (optional)
-    const uint32_t* alias_index;
+    // alias-table sampling (optional; a render that asks for it also points env_pdf at the
+    // alias sampler's own texel densities)
+    const unsigned long long* alias_threshold;  // [column] 48-bit residual threshold
+    const uint32_t* alias_index;                // [column] alias texel
 };
 
 // Per-render constants (camera basis from Camera::generate, geometry.cpp:219-224).
@@ -119,6 +121,14 @@ struct GuidePathRefs {
     int32_t record = 0;                      // collect training samples
 };
 
+// Diagnostic record of every traced ray (cr_gpu_render_trace_dump); null otherwise. Only the
+// counting traversal kernels write it.
+struct TraceDump {
+    cr_traced_ray* rays = nullptr;
+    unsigned long long* count = nullptr;
+    uint64_t capacity = 0;
+};
+
 // Path state, structure of arrays over path slots.
 struct PathSoA {
     float4* ray_o;        // origin, tmin
@@ -143,6 +153,7 @@ struct PathSoA {
     // per-sample radiance of the current chunk, indexed by sample id - chunk start
     float4* out;
     GuidePathRefs guide;  // zero unless the render is guided
+    TraceDump dump;       // zero unless the render records its rays
 };
 // bits of PathSoA::flags
 enum : uint32_t { kPathLastDelta = 1u, kPathPrecise = 2u, kPathDead = 4u, kPathShadow = 8u };

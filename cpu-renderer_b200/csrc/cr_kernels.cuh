@@ -434,6 +434,24 @@ CR_D int closestFinish(const DevScene& S, const RenderParams& P, const PathSoA& 
     return (S.nee_skip && (h.flags & kTriNeeNull)) ? kShadeNeeNull : kShadeGeneric;
 }
 
+// Records one traced ray and the traversal's answer (cr_gpu_render_trace_dump).
+CR_D void dumpRay(const TraceDump& D, const TRay& r, uint32_t ignore, uint32_t kind, uint32_t depth, bool found,
+                  const HitRec& h) {
+    const unsigned long long i = atomicAdd(D.count, 1ull);
+    if (i >= D.capacity) return;
+    cr_traced_ray& o = D.rays[i];
+    o.ray.origin[0] = r.o.x; o.ray.origin[1] = r.o.y; o.ray.origin[2] = r.o.z;
+    o.ray.direction[0] = r.d.x; o.ray.direction[1] = r.d.y; o.ray.direction[2] = r.d.z;
+    o.ray.tmin = r.tmin; o.ray.tmax = r.tmax;
+    o.ray.origin_low[0] = r.olow.x; o.ray.origin_low[1] = r.olow.y; o.ray.origin_low[2] = r.olow.z;
+    o.ignore = ignore; o.kind = kind; o.depth = depth; o.found = found ? 1u : 0u;
+    o.hit.t = found ? h.t : static_cast<double>(kInf);
+    o.hit.u = found ? h.u : 0.0;
+    o.hit.v = found ? h.v : 0.0;
+    o.hit.triangle = found ? h.tri : kNoTriangle;
+    o.hit.reserved_ = 0;
+}
+
 // Any hit for one queued shadow ray; an unoccluded contribution is added (render.cpp:283-296).
 // Returns true when the path had ended and its slot is now free.
 template <bool COUNT = false, bool NOALPHA = false>
@@ -451,6 +469,7 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
     if (COUNT) {
         atomicAdd(&stats[kStatShadowPairs], static_cast<unsigned long long>(vc.pairs));
         atomicAdd(&stats[kStatShadowTris], static_cast<unsigned long long>(vc.tris));
+        if (st.dump.rays) dumpRay(st.dump, r, __float_as_uint(lo.w), 1, st.depth[path], blocked, h);
     }
     return shadowFinish(P, O, st, path, E, blocked, err, c);
 }
@@ -469,6 +488,7 @@ CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st,
     if (COUNT) {
         atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
         atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
+        if (st.dump.rays) dumpRay(st.dump, r, st.prev_tri[path], 0, st.depth[path], found, h);
     }
     return closestFinish(S, P, st, path, E, found, h, err);
 }
@@ -735,6 +755,19 @@ static __global__ void k_intersect_batch(DevScene S, const cr_ray* rays, cr_hit*
         if (f) { cr_hit out = in; out.t = h.t; out.u = h.u; out.v = h.v; out.triangle = h.tri; hits[i] = out; }
         found[i] = f ? 1 : 0;
         if (err) atomicMin(errIndex, static_cast<unsigned long long>(i));
+    }
+}
+
+// Environment samples for checks of the sampler: texel and density of sample i of the stream
+// Rng(sampleSeed(seed, i, 0)). S.env_pdf holds the densities of the sampler in use.
+static __global__ void k_env_samples(DevScene S, int alias, uint64_t seed, uint64_t first, uint64_t count,
+                                     uint32_t* texels, float* densities) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        Rng rng(sampleSeed(seed, first + i, 0));
+        const uint64_t index = envPickTexel(S, rng, alias != 0);
+        texels[i] = static_cast<uint32_t>(index);
+        densities[i] = __ldg(S.env_pdf + index);
     }
 }
 

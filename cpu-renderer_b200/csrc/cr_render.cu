@@ -528,7 +528,7 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
     if (E.hasImage) {
         S.env_width = E.width; S.env_height = E.height;
         S.env_coarse_count = static_cast<uint32_t>(E.coarse.size());
-        S.alias_prob = nullptr;  // built on the first render that asks for alias sampling
+        S.alias_threshold = nullptr;  // built on the first render that asks for alias sampling
         S.alias_index = nullptr;
     }
     S.env_weight_sum = E.weightSum;
@@ -577,10 +577,21 @@ struct GuideRun {
     uint32_t epochs = 4;
 };
 
+// The alias-table sampler's tables, built and uploaded on the first request (scene with an
+// environment image only).
+void ensureAlias(cr_gpu_scene& g) {
+    if (!g.dev.env_has_image || g.dev.alias_threshold) return;
+    crh::build_alias(g.env);
+    g.dev.alias_threshold = reinterpret_cast<const unsigned long long*>(
+        g.aliasAlloc.upload(g.env.aliasThreshold.data(), g.env.aliasThreshold.size(), g.stream));
+    g.dev.alias_index = g.aliasAlloc.upload(g.env.aliasIndex.data(), g.env.aliasIndex.size(), g.stream);
+    g.aliasPdf = g.aliasAlloc.upload(g.env.aliasPdf.data(), g.env.aliasPdf.size(), g.stream);
+}
+
 // The whole render. filmHost may be NULL (film stays on the device).
 void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, cr_progress_fn progress,
                 void* user, float* filmHost, cr_render_stats* stats, const cr_gpu_tuning& tuning, float* perSample,
-                const Frames& frames = Frames{}, const GuideRun* guide = nullptr) {
+                const Frames& frames = Frames{}, const GuideRun* guide = nullptr, const TraceDump* dump = nullptr) {
     const auto start = std::chrono::steady_clock::now();
     crh::validate_options(o);
     const uint64_t pixels = static_cast<uint64_t>(o.width) * o.height;
@@ -642,6 +653,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         ~ReleaseAtEnd() { cudaStreamSynchronize(s); m.release(); }
     } releaseGuide{guideMem, g.stream};
     PathSoA st = W.st;  // after the workspace buffers above exist
+    if (dump) st.dump = *dump;  // recorded by the counting traversal kernels
     const uint64_t trainTotal = guide ? std::min<uint64_t>(total, static_cast<uint64_t>(guide->trainSamples) * pixels) : 0;
     float* guideOut = nullptr;
     GuideSample* guideSamples = nullptr;
@@ -667,8 +679,8 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         st.guide.record = 1;
         CR_CUDA(cudaMemsetAsync(st.guide.sampleCount, 0, sizeof(unsigned long long), g.stream));
     }
-    if (!W.hostCounts) CR_CUDA(cudaMallocHost(&W.hostCounts, kCountWords * sizeof(uint32_t)));
-    if (!W.hostStats) CR_CUDA(cudaMallocHost(&W.hostStats, kStatWords * sizeof(unsigned long long)));
+    if (!W.hostCounts) { crh::count_allocation(); CR_CUDA(cudaMallocHost(&W.hostCounts, kCountWords * sizeof(uint32_t))); }
+    if (!W.hostStats) { crh::count_allocation(); CR_CUDA(cudaMallocHost(&W.hostStats, kStatWords * sizeof(unsigned long long))); }
     cudaStream_t s = g.stream;
     if (!W.gridTrace) {
         W.gridTrace = occupancyGrid(reinterpret_cast<const void*>(k_trace<false>), 128, g.device);
@@ -684,11 +696,13 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
         W.gridSmall = sms * 8;
     }
-    if (tuning.env_alias && g.dev.env_has_image && !g.dev.alias_prob) {  // built on first request
-        crh::build_alias(g.env);
-        g.dev.alias_prob = g.aliasAlloc.upload(g.env.aliasProb.data(), g.env.aliasProb.size(), s);
-        g.dev.alias_index = g.aliasAlloc.upload(g.env.aliasIndex.data(), g.env.aliasIndex.size(), s);
-    }
+    if (tuning.env_alias) ensureAlias(g);
+    // The scene as this render's kernels see it: alias sampling reads the alias sampler's own
+    // texel densities (for light samples and MIS weights alike); the diagnostic switch
+    // generic_shading sends every hit through the generic shading kernel.
+    DevScene dev = g.dev;
+    if (tuning.env_alias && g.dev.env_has_image) dev.env_pdf = g.aliasPdf;
+    if (tuning.generic_shading) dev.nee_skip = 0;
     CR_CUDA(cudaMemsetAsync(g.acc, 0, 3 * pixels * sizeof(double), s));
     CR_CUDA(cudaMemsetAsync(W.stats, 0, kStatWords * sizeof(unsigned long long), s));
     const unsigned long long noError = ~0ull;
@@ -746,11 +760,11 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     if (timePhases) { CR_CUDA(cudaEventRecord(W.event(ev + 1), s)); timed.push_back({ev, phase}); ev += 2; }
                     ++launches;
                 };
-                rec(2, [&] { k_regen<false><<<cap(W.gridRegen), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
+                rec(2, [&] { k_regen<false><<<cap(W.gridRegen), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}, 1); });
                 rec(0, [&] {
-                    if (tuning.count_traversal) k_trace<true><<<cap(W.gridTrace), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                    else if (noAlpha) k_trace<false, false, true><<<cap(W.gridTraceNoAlpha), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                    else k_trace<false><<<cap(W.gridTrace), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    if (tuning.count_traversal) k_trace<true><<<cap(W.gridTrace), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    else if (noAlpha) k_trace<false, false, true><<<cap(W.gridTraceNoAlpha), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                    else k_trace<false><<<cap(W.gridTrace), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                 });
                 // shading: the lean instantiations when the scene allows them. The classes'
                 // queues are independent, so without phase timing or guiding the miss and
@@ -760,13 +774,13 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     CR_CUDA(cudaEventRecord(W.fork, s));
                     for (int k = 0; k < 2; ++k) CR_CUDA(cudaStreamWaitEvent(W.side[k], W.fork, 0));
                     if (lean) {
-                        k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, W.side[0]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                        k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, W.side[1]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                        k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, W.side[0]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, W.side[1]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                     } else {
-                        k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, W.side[0]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                        k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, W.side[1]>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
-                        k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, W.side[0]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, W.side[1]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                     }
                     for (int k = 0; k < 2; ++k) {
                         CR_CUDA(cudaEventRecord(W.join[k], W.side[k]));
@@ -775,25 +789,25 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                     launches += 3;
                 } else {
                 if (lean) {
-                    rec(1, [&] { k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
-                    rec(1, [&] { k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else {
-                    rec(1, [&] { k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
-                    rec(1, [&] { k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 }
                 if (guide) {
                     rec(1, [&] {
                         guideInferPaths(guide->gd, s, W.q.shade[kShadeGeneric], W.q.counts + kCountShade0 + kShadeGeneric,
-                                        static_cast<uint32_t>(pool), st, st.guide.hitT, g.dev,
+                                        static_cast<uint32_t>(pool), st, st.guide.hitT, dev,
                                         V3{st.guide.lo[0], st.guide.lo[1], st.guide.lo[2]},
                                         V3{st.guide.inv[0], st.guide.inv[1], st.guide.inv[2]}, guideOut);
                     });
-                    if (lean) rec(1, [&] { k_shade<kShadeGeneric, false, true, true><<<cap(W.gridShadeLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
-                    else rec(1, [&] { k_shade<kShadeGeneric, false, true><<<cap(W.gridShade), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    if (lean) rec(1, [&] { k_shade<kShadeGeneric, false, true, true><<<cap(W.gridShadeLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    else rec(1, [&] { k_shade<kShadeGeneric, false, true><<<cap(W.gridShade), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else if (lean) {
-                    rec(1, [&] { k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else {
-                    rec(1, [&] { k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(g.dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    rec(1, [&] { k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 }
                 }
                 cur ^= 1;
@@ -869,7 +883,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         CR_CUDA(cudaStreamSynchronize(s));
         CR_CUDA(cudaMemsetAsync(W.detail, 0, sizeof(DevError), s));
         CR_CUDA(cudaMemsetAsync(W.stats, 0, 2 * sizeof(unsigned long long), s));
-        k_trace_one<<<1, 32, 0, s>>>(g.dev, P, W.st, y * static_cast<uint32_t>(o.width) + x, sample, W.detail, W.stats, W.stats + 1);
+        k_trace_one<<<1, 32, 0, s>>>(dev, P, W.st, y * static_cast<uint32_t>(o.width) + x, sample, W.detail, W.stats, W.stats + 1);
         CR_CUDA(cudaMemcpyAsync(&host, W.detail, sizeof(DevError), cudaMemcpyDeviceToHost, s));
         CR_CUDA(cudaStreamSynchronize(s));
         if (!host.code) { host.code = -1; host.x = static_cast<int32_t>(x); host.y = static_cast<int32_t>(y); host.sample = static_cast<int32_t>(sample); }
@@ -961,20 +975,30 @@ size_t layoutNoAlloc(unsigned char* base, NoAllocLayout& L) {
     return off;
 }
 
-// Device address of the workspace, looked up once per device (cudaGetSymbolAddress) with that
-// device current; the host-side name of the array is not a device address.
-unsigned char* noallocBase(int device) {
+// Per-device set-up of the allocation-free render: the workspace's device address, looked up
+// once per device (cudaGetSymbolAddress) with that device current (the host-side name of the
+// array is not a device address), and two timing events. The address is cached for the life of
+// the process: a host that calls cudaDeviceReset would invalidate it, and must not call
+// cr_gpu_render_noalloc on that device afterwards.
+struct NoAllocDevice {
+    unsigned char* base = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+};
+const NoAllocDevice& noallocDevice(int device) {
     static std::mutex m;
-    static unsigned char* addr[64] = {};
+    static NoAllocDevice dev[64];
     if (device < 0 || device >= 64) throw crh::Error(CR_ERR_INVALID_ARGUMENT, "device index out of range");
     std::lock_guard<std::mutex> lock(m);
-    if (!addr[device]) {
+    NoAllocDevice& d = dev[device];
+    if (!d.base) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
         if (e != cudaSuccess) throw CudaError(e, "cudaGetSymbolAddress(g_noallocScratch)");
-        addr[device] = static_cast<unsigned char*>(p);
+        CR_CUDA(cudaEventCreate(&d.start));
+        CR_CUDA(cudaEventCreate(&d.stop));
+        d.base = static_cast<unsigned char*>(p);
     }
-    return addr[device];
+    return d;
 }
 
 void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_options& o, float* filmHost,
@@ -996,15 +1020,25 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
     CR_CUDA(cudaSetDevice(g.device));
     NoAllocLayout L;
     if (layoutNoAlloc(nullptr, L) > kNoAllocBytes) throw crh::Error(CR_ERR_LOGIC, "no-alloc workspace layout exceeds its array");
-    layoutNoAlloc(noallocBase(g.device), L);
+    const NoAllocDevice& D = noallocDevice(g.device);
+    layoutNoAlloc(D.base, L);
     cudaStream_t s = g.stream;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
-    const int gridTrace = occupancyGrid(reinterpret_cast<const void*>(k_trace<false>), 128, g.device);
-    const int gridShade = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric>), 128, g.device);
-    const int gridLight = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull>), 128, g.device);
-    const int gridMiss = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss>), 128, g.device);
+    // the kernel variants cr_gpu_render picks for this scene (host-side choices only): the
+    // traversal without the alpha test when no triangle is alpha-masked, the lean shading
+    // kernels without textures, punctual lights or alpha masks
+    const bool noAlpha = !g.dev.any_alpha_mask;
+    const bool lean = g.dev.texture_count == 0 && g.dev.punctual_count == 0 && !g.dev.any_alpha_mask;
+    const void* traceK = noAlpha ? reinterpret_cast<const void*>(k_trace<false, false, true>) : reinterpret_cast<const void*>(k_trace<false>);
+    const void* shadeK[kShadeClasses] = {
+        lean ? reinterpret_cast<const void*>(k_shade<kShadeMiss, false, false, true>) : reinterpret_cast<const void*>(k_shade<kShadeMiss>),
+        lean ? reinterpret_cast<const void*>(k_shade<kShadeNeeNull, false, false, true>) : reinterpret_cast<const void*>(k_shade<kShadeNeeNull>),
+        lean ? reinterpret_cast<const void*>(k_shade<kShadeGeneric, false, false, true>) : reinterpret_cast<const void*>(k_shade<kShadeGeneric>)};
     const int gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen<false>), 128, g.device);
+    const int gridTrace = occupancyGrid(traceK, 128, g.device);
+    int gridShadeK[kShadeClasses];
+    for (int c = 0; c < kShadeClasses; ++c) gridShadeK[c] = occupancyGrid(shadeK[c], 128, g.device);
     const int gridSmall = sms * 8;
     // The workspace keeps the previous call's contents: clear what must start at zero.
     CR_CUDA(cudaMemsetAsync(L.acc, 0, 3 * pixels * sizeof(double), s));
@@ -1019,6 +1053,10 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
     const uint64_t chunk = std::min<uint64_t>(total, kNoAllocChunk);
     uint64_t iterations = 0, launches = 0;
     bool errored = false;
+    // no launch needs more blocks than the pool has 128-path batches
+    const int poolBlocks = static_cast<int>((pool + 127) / 128);
+    auto cap = [&](int grid) { return std::max(1, std::min(grid, poolBlocks)); };
+    CR_CUDA(cudaEventRecord(D.start, s));
     for (uint64_t c0 = 0; c0 < total && !errored; c0 += chunk) {
         const Chunk C{c0, std::min<uint64_t>(total, c0 + chunk), pixels};
         CR_CUDA(cudaMemsetAsync(L.q.counts, 0, kCountWords * sizeof(uint32_t), s));
@@ -1031,11 +1069,18 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
         int cur = 0;
         for (;;) {
             for (int b = 0; b < 8; ++b) {
-                k_regen<false><<<gridRegen, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{}, 1);
-                k_trace<false><<<gridTrace, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
-                k_shade<kShadeMiss><<<gridMiss, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
-                k_shade<kShadeNeeNull><<<gridLight, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
-                k_shade<kShadeGeneric><<<gridShade, 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                k_regen<false><<<cap(gridRegen), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{}, 1);
+                if (noAlpha) k_trace<false, false, true><<<cap(gridTrace), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                else k_trace<false><<<cap(gridTrace), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                if (lean) {
+                    k_shade<kShadeMiss, false, false, true><<<cap(gridShadeK[0]), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                    k_shade<kShadeNeeNull, false, false, true><<<cap(gridShadeK[1]), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                    k_shade<kShadeGeneric, false, false, true><<<cap(gridShadeK[2]), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                } else {
+                    k_shade<kShadeMiss><<<cap(gridShadeK[0]), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                    k_shade<kShadeNeeNull><<<cap(gridShadeK[1]), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                    k_shade<kShadeGeneric><<<cap(gridShadeK[2]), 128, 0, s>>>(g.dev, P, L.st, L.q, cur, C, E, L.stats, JobTable{});
+                }
                 launches += 5;
                 cur ^= 1;
                 ++iter;
@@ -1072,13 +1117,22 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
     }
     k_film<<<gridSmall, 128, 0, s>>>(L.acc, L.film, pixels, o.samples);
     ++launches;
+    CR_CUDA(cudaEventRecord(D.stop, s));
     if (filmHost) CR_CUDA(cudaMemcpyAsync(filmHost, L.film, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaMemcpyAsync(hostStats, L.stats, sizeof(hostStats), cudaMemcpyDeviceToHost, s));
     CR_CUDA(cudaStreamSynchronize(s));
     CR_CUDA(cudaGetLastError());
+    float deviceMs = 0;
+    CR_CUDA(cudaEventElapsedTime(&deviceMs, D.start, D.stop));
     if (stats) {
+        // as cr_gpu_render fills them, except trace_ms/shade_ms/regen_ms (no phase timing here)
         std::memset(stats, 0, sizeof(*stats));
         stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+        stats->device_ms = deviceMs;
+        stats->extend_pairs = hostStats[kStatPairs];
+        stats->extend_triangles = hostStats[kStatTris];
+        stats->shadow_pairs = hostStats[kStatShadowPairs];
+        stats->shadow_triangles = hostStats[kStatShadowTris];
         stats->workers = referenceWorkers(o);
         stats->chunks = static_cast<int32_t>((total + chunk - 1) / chunk);
         stats->camera_samples = total;
@@ -1094,6 +1148,12 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
 }  // namespace
 
 extern "C" {
+
+cr_status cr_gpu_allocation_count(uint64_t* count) {
+    if (!count) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "count is NULL");
+    *count = crh::allocation_count();
+    return CR_OK;
+}
 
 cr_status cr_gpu_device_count(int* count) {
     int n = 0;
@@ -1207,6 +1267,73 @@ cr_status cr_gpu_render_resident(cr_gpu_scene* g, const cr_camera* camera, const
         if (!g || !camera || !options) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
         std::lock_guard<std::mutex> lock(g->mutex);
         renderImpl(*g, *camera, *options, nullptr, nullptr, nullptr, stats, defaults(tuning), per_sample_rgb);
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+static_assert(sizeof(cr_traced_ray) == 96, "cr_traced_ray layout");
+
+cr_status cr_gpu_environment_sample(cr_gpu_scene* g, int alias, uint64_t seed, uint64_t count, uint32_t* texels,
+                                    float* densities) {
+    try {
+        if (!g || (count && (!texels || !densities))) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        if (!g->dev.env_has_image) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "the scene has no environment image");
+        CR_CUDA(cudaSetDevice(g->device));
+        if (alias) ensureAlias(*g);
+        DevScene dev = g->dev;
+        if (alias) dev.env_pdf = g->aliasPdf;
+        DevAlloc mem;
+        struct Release {
+            DevAlloc& m;
+            cudaStream_t s;
+            ~Release() { cudaStreamSynchronize(s); m.release(); }
+        } release{mem, g->stream};
+        const uint64_t batch = std::min<uint64_t>(std::max<uint64_t>(count, 1), uint64_t{1} << 26);
+        uint32_t* dTex = mem.alloc<uint32_t>(batch);
+        float* dPdf = mem.alloc<float>(batch);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+        for (uint64_t b = 0; b < count; b += batch) {  // sample i of the call uses stream i
+            const uint64_t m = std::min<uint64_t>(batch, count - b);
+            k_env_samples<<<sms * 8, 128, 0, g->stream>>>(dev, alias, seed, b, m, dTex, dPdf);
+            CR_CUDA(cudaGetLastError());
+            CR_CUDA(cudaMemcpyAsync(texels + b, dTex, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
+            CR_CUDA(cudaMemcpyAsync(densities + b, dPdf, m * sizeof(float), cudaMemcpyDeviceToHost, g->stream));
+            CR_CUDA(cudaStreamSynchronize(g->stream));
+        }
+        return CR_OK;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+cr_status cr_gpu_render_trace_dump(cr_gpu_scene* g, const cr_camera* camera, const cr_render_options* options,
+                                   const cr_gpu_tuning* tuning, cr_traced_ray* rays, uint64_t capacity, uint64_t* count) {
+    try {
+        if (!g || !camera || !options || !count || (capacity && !rays))
+            return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        std::lock_guard<std::mutex> lock(g->mutex);
+        CR_CUDA(cudaSetDevice(g->device));
+        cr_gpu_tuning t = defaults(tuning);
+        t.count_traversal = 1;  // the counting kernels record the rays
+        DevAlloc mem;
+        struct Release {
+            DevAlloc& m;
+            cudaStream_t s;
+            ~Release() { cudaStreamSynchronize(s); m.release(); }
+        } release{mem, g->stream};
+        TraceDump d;
+        d.capacity = capacity;
+        d.rays = mem.alloc<cr_traced_ray>(capacity ? capacity : 1);
+        d.count = mem.alloc<unsigned long long>(1);
+        CR_CUDA(cudaMemsetAsync(d.count, 0, sizeof(unsigned long long), g->stream));
+        renderImpl(*g, *camera, *options, nullptr, nullptr, nullptr, nullptr, t, nullptr, Frames{}, nullptr, &d);
+        unsigned long long n = 0;
+        CR_CUDA(cudaMemcpyAsync(&n, d.count, sizeof(n), cudaMemcpyDeviceToHost, g->stream));
+        CR_CUDA(cudaStreamSynchronize(g->stream));
+        const uint64_t copy = std::min<uint64_t>(n, capacity);
+        if (copy) CR_CUDA(cudaMemcpyAsync(rays, d.rays, copy * sizeof(cr_traced_ray), cudaMemcpyDeviceToHost, g->stream));
+        CR_CUDA(cudaStreamSynchronize(g->stream));
+        *count = n;
         return CR_OK;
     } catch (const std::exception& e) { return fail(e); }
 }

@@ -405,6 +405,29 @@ CR_D uint32_t envUpperBound(const DevScene& S, double pick) {
     }
     return static_cast<uint32_t>(lo);
 }
+// The texel an environment-image sample takes (Environment::sample's first step,
+// render.cpp:73-75, or the alias table).
+CR_D uint64_t envPickTexel(const DevScene& S, Rng& rng, bool alias) {
+    const uint64_t n = static_cast<uint64_t>(S.env_width) * S.env_height;
+    uint64_t index;
+    if (alias && S.alias_threshold) {
+        // Walker's alias method (Walker 1977; Vose 1991). Two draws form a 48-bit uniform x;
+        // x*n = col*2^48 + r gives the column and a 48-bit residual that chooses between the
+        // column and its alias (the host set the thresholds so that every texel's probability
+        // is an exact count over 2^48, and env_pdf holds those densities). A different stream
+        // from the CDF search: used only when alias sampling is requested.
+        const uint64_t a = rng.next() >> 8, b = rng.next() >> 8;
+        const uint64_t xs = ((a << 24) | b) << 16;
+        const uint64_t col = __umul64hi(xs, n);        // < n: x < 2^48
+        const uint64_t r = (xs * n) >> 16;            // (x*n) mod 2^48
+        index = r < __ldg(S.alias_threshold + col) ? col : __ldg(S.alias_index + col);
+    } else {
+        const double pick = rng.uniform() * S.env_weight_sum;
+        index = envUpperBound(S, pick);
+        if (index > n - 1) index = n - 1;
+    }
+    return index;
+}
 CR_D V3 envSample(const DevScene& S, Rng& rng, float& density, bool alias) {
     if (!S.env_has_image) {
         const float y = 1 - 2 * rng.uniform(), phi = 2 * kPi * rng.uniform(), r = sqrtf(smax(0.0f, 1 - y * y));
@@ -413,24 +436,7 @@ CR_D V3 envSample(const DevScene& S, Rng& rng, float& density, bool alias) {
         fsincos(phi, sp, cp);
         return {r * cp, y, r * sp};
     }
-    const uint64_t n = static_cast<uint64_t>(S.env_width) * S.env_height;
-    uint64_t index;
-    if (alias && S.alias_prob) {
-        // Walker's alias method (Walker 1977; Vose 1991). Two draws form a 48-bit fixed-point
-        // uniform; its product with n gives the column and a 24-bit residual that chooses
-        // between the column and its alias. A different stream from the CDF search: used
-        // only when alias sampling is requested.
-        const uint64_t a = rng.next() >> 8, b = rng.next() >> 8;
-        const uint64_t xs = ((a << 24) | b) << 16;
-        uint64_t col = __umul64hi(xs, n);
-        if (col >= n) col = n - 1;
-        const float frac = static_cast<float>((xs * n) >> 40) * (1.0f / 16777216.0f);
-        index = frac < __ldg(S.alias_prob + col) ? col : __ldg(S.alias_index + col);
-    } else {
-        const double pick = rng.uniform() * S.env_weight_sum;
-        index = envUpperBound(S, pick);
-        if (index > n - 1) index = n - 1;
-    }
+    const uint64_t index = envPickTexel(S, rng, alias);
     const int W = S.env_width, H = S.env_height;
     const int x = static_cast<int>(index % W), y = static_cast<int>(index / W);
     const float u = (static_cast<float>(x) + rng.uniform()) / static_cast<float>(W);
@@ -535,7 +541,7 @@ CR_D void skipLight(const DevScene& S, Rng& rng, bool alias) {
     }
     const uint32_t type = S.light_entries[lo == S.light_entry_count ? S.light_entry_count - 1 : lo].type;
     int draws = 0;
-    if (type == kLightEnvironment) draws = !S.env_has_image ? 2 : (alias && S.alias_prob ? 4 : 3);
+    if (type == kLightEnvironment) draws = !S.env_has_image ? 2 : (alias && S.alias_threshold ? 4 : 3);
     else if (type == kLightTriangle) draws = 2;
     for (int k = 0; k < draws; ++k) rng.next();
 }

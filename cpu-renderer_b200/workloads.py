@@ -28,7 +28,7 @@ import math
 
 import numpy as np
 
-from crgpu import Camera, Options, new_materials, new_triangles
+from cr_types import Camera, Options, new_materials, new_triangles
 
 ROOM_SEED = 0x5EED0001
 GRID_SEED = 0x5EED0002

@@ -224,7 +224,8 @@ typedef struct cr_gpu_tuning {
     int32_t env_alias;         /* 1: alias-table environment sampling (different streams)   */
     int32_t paths_per_wave;    /* 0: automatic                                             */
     int32_t chunk_log2;        /* 0: automatic; n in [16, 28]: 2^n sample ids per chunk     */
-    int32_t reserved;          /* must be 0                                                */
+    int32_t generic_shading;   /* 1: every hit through the generic shading kernel (no
+                                  NEE-null class; diagnostic: the films are identical)    */
     int32_t time_phases;       /* 1: CUDA-event time every extend/shade/shadow launch      */
     int32_t count_traversal;   /* 1: count node pairs and triangles visited by closest-hit */
 } cr_gpu_tuning;
@@ -296,6 +297,35 @@ cr_status cr_gpu_render_resident(cr_gpu_scene* scene, const cr_camera* camera,
                                  const cr_gpu_tuning* tuning, float* per_sample_rgb);
 cr_status cr_gpu_film_download(cr_gpu_scene* scene, float* film_rgb, uint64_t floats);
 
+/* Environment samples (diagnostic; no counterpart in the reference): the texel and density of
+ * `count` samples of the environment image, sample i from the stream
+ * Rng(sampleSeed(seed, i, 0)), by the reference's CDF search (Environment::sample,
+ * render.cpp:67-84; alias = 0) or by the alias table (alias = 1), whose densities are its own
+ * realised texel probabilities over the texel's solid angle. For checks of the sampler's
+ * distribution. */
+cr_status cr_gpu_environment_sample(cr_gpu_scene* scene, int alias, uint64_t seed, uint64_t count,
+                                    uint32_t* texels, float* densities);
+
+/* One ray a render traced and the traversal's answer (diagnostic; no counterpart in the
+ * reference, whose trace() calls Bvh::intersect, geometry.cpp:554-639, with exactly these
+ * arguments: render.cpp:241 for kind 0, render.cpp:284-285 for kind 1). */
+typedef struct cr_traced_ray {
+    cr_ray ray;
+    uint32_t ignore;    /* the query's ignoreTriangle                                        */
+    uint32_t kind;      /* 0: closest hit (any = false), 1: shadow ray (any = true)          */
+    uint32_t depth;     /* the path's bounce when the ray was traced                         */
+    uint32_t found;     /* the traversal's return value                                      */
+    cr_hit hit;         /* kind 0 and found: t, u, v, triangle as the traversal returned them */
+} cr_traced_ray;
+
+/* As cr_gpu_render_resident (counting traversal kernels, no per-sample output), and every ray
+ * the render traces is recorded: the first `capacity` of them (in no particular order) go to
+ * rays, *count receives how many were traced. For parity checks of the traversal on the rays
+ * a real render produces, bounce by bounce. */
+cr_status cr_gpu_render_trace_dump(cr_gpu_scene* scene, const cr_camera* camera,
+                                   const cr_render_options* options, const cr_gpu_tuning* tuning,
+                                   cr_traced_ray* rays, uint64_t capacity, uint64_t* count);
+
 /* cr_gpu_render without any allocation (no counterpart in the reference).
  *
  * For callers that cannot allocate device memory while rendering: hosts that hand out GPU
@@ -310,14 +340,24 @@ cr_status cr_gpu_film_download(cr_gpu_scene* scene, float* film_rgb, uint64_t fl
  * Limits: width*height <= 262144 (512x512); any sample and bounce counts cr::RenderOptions
  * accepts. Larger images fail with CR_ERR_INVALID_ARGUMENT before any work.
  *
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress), so
- * make that first call before any stream capture. All calls on a device share the array and
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) and
+ * creates two timing events, so make that first call before any stream capture. Under the CUDA
+ * runtime's lazy module loading (the default since CUDA 12.2) the array is committed on a device
+ * when this library's render module first loads there, which can be that first call: make one
+ * small call at start-up, while memory is still to be had, and the later calls reserve nothing.
+ * stats, when not NULL, is filled as cr_gpu_render fills it, except trace_ms, shade_ms and
+ * regen_ms, which stay 0. All calls on a device share the array and
  * it keeps the last call's contents (each call clears what must start at zero); calls that
  * overlap on the GPU — from different threads or scenes on one device — race on it and must
  * be serialised by the caller. */
 cr_status cr_gpu_render_noalloc(cr_gpu_scene* scene, const cr_camera* camera,
                                 const cr_render_options* options, float* film_rgb,
                                 cr_render_stats* stats);
+
+/* Diagnostic (no counterpart in the reference): the number of memory blocks this library has
+ * requested since it was loaded, device blocks (cudaMalloc or its own block cache) and
+ * page-locked host blocks alike. A call that allocates nothing leaves it unchanged. */
+cr_status cr_gpu_allocation_count(uint64_t* count);
 
 /* ---- output encoding on the device ----------------------------------------------------------
  * Replaces the per-pixel work of io::writePng / io::writeHdr (src/io/image.cpp:100-124,

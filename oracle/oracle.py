@@ -14,7 +14,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "cpu-renderer_b200"))
-from crgpu import (Camera, EnvDesc, Image, Options, SceneDesc, hit_dtype, light_dtype, material_dtype,  # noqa: E402
+from cr_types import (Camera, EnvDesc, Image, Options, SceneDesc, hit_dtype, light_dtype, material_dtype,  # noqa: E402
                    node_dtype, ray_dtype, texture_dtype, triangle_dtype, INF, NO_TRIANGLE)
 
 LIB_PATH = os.path.join(HERE, "liboracle.so")

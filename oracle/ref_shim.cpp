@@ -12,12 +12,14 @@
 #include "render.h"
 #include "cr_gpu.h"
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <memory>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <typeinfo>
 #include <vector>
 
@@ -215,6 +217,34 @@ int ref_intersect(const void* s, const void* b, const cr_ray* rays, uint64_t n, 
             found[i] = bvh.intersect(scene, ray(rays[i]), h, any != 0, ignore) ? 1 : 0;
             std::memcpy(&hits[i], &h, sizeof(h));
         }
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+// Bvh::intersect over rays that each carry their own ignoreTriangle (the rays a render
+// traced), split across `threads` host threads.
+int ref_intersect_rays(const void* s, const void* b, const cr_ray* rays, const uint32_t* ignores, uint64_t n,
+                       int any, cr_hit* hits, uint8_t* found, int threads) {
+    try {
+        const auto& scene = *static_cast<const cr::Scene*>(s);
+        const auto& bvh = *static_cast<const cr::Bvh*>(b);
+        const uint64_t workers = std::max<uint64_t>(1, std::min<uint64_t>(threads > 0 ? threads : 1, n));
+        std::vector<std::thread> pool;
+        std::vector<std::string> errors(workers);
+        for (uint64_t w = 0; w < workers; ++w) {
+            pool.emplace_back([&, w] {
+                try {
+                    for (uint64_t i = w; i < n; i += workers) {
+                        cr::Hit h;
+                        std::memcpy(&h, &hits[i], sizeof(h));
+                        found[i] = bvh.intersect(scene, ray(rays[i]), h, any != 0, ignores[i]) ? 1 : 0;
+                        std::memcpy(&hits[i], &h, sizeof(h));
+                    }
+                } catch (const std::exception& e) { errors[w] = e.what(); }
+            });
+        }
+        for (auto& t : pool) t.join();
+        for (auto& e : errors)
+            if (!e.empty()) throw std::runtime_error(e);
         return 0;
     } catch (const std::exception& e) { return fail(e); }
 }

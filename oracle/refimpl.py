@@ -13,7 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(ROOT, "cpu-renderer_b200"))
-from crgpu import (Camera, EnvDesc, Options, SceneDesc, Stats, hit_dtype, light_dtype, material_dtype,  # noqa: E402
+from cr_types import (Camera, EnvDesc, Options, SceneDesc, Stats, hit_dtype, light_dtype, material_dtype,  # noqa: E402
                    node_dtype, ray_dtype, triangle_dtype, texture_dtype, Image, INF, NO_TRIANGLE)
 
 LIB_PATH = os.path.join(HERE, "_ref", "libcr_ref.so")
@@ -45,6 +45,7 @@ def lib():
             "ref_bvh_node_count": (C.c_uint64, [P]),
             "ref_bvh_export": (None, [P, P, P]),
             "ref_intersect": (C.c_int, [P, P, P, C.c_uint64, C.c_int, C.c_uint32, P, P]),
+            "ref_intersect_rays": (C.c_int, [P, P, P, P, C.c_uint64, C.c_int, P, P, C.c_int]),
             "ref_intersect_triangle": (C.c_int, [P, P, P]),
             "ref_bounds_intersect": (C.c_int, [P, P, P, C.POINTER(C.c_float)]),
             "ref_camera_generate": (C.c_int, [C.POINTER(Camera), P, P, C.c_uint64, C.c_int, C.c_int, P]),
@@ -153,6 +154,21 @@ class RefScene:
         hits = np.ascontiguousarray(hits, dtype=hit_dtype).copy()
         found = np.zeros(n, np.uint8)
         code = lib().ref_intersect(self.handle, self.bvh, _ptr(rays), n, int(any_hit), ignore, _ptr(hits), _ptr(found))
+        if code:
+            _err(code)
+        return found.astype(bool), hits
+
+    def intersect_rays(self, rays, ignores, any_hit=False, threads=None):
+        """Bvh::intersect of every ray with its own ignoreTriangle, on several host threads;
+        the incoming hit is the reference's default (t = +inf)."""
+        rays = np.ascontiguousarray(rays, dtype=ray_dtype)
+        ignores = np.ascontiguousarray(ignores, dtype=np.uint32)
+        n = len(rays)
+        hits = np.zeros(n, hit_dtype)
+        hits["t"] = INF
+        found = np.zeros(n, np.uint8)
+        code = lib().ref_intersect_rays(self.handle, self.bvh, _ptr(rays), _ptr(ignores), n, int(any_hit), _ptr(hits),
+                                        _ptr(found), int(threads or os.cpu_count() or 1))
         if code:
             _err(code)
         return found.astype(bool), hits

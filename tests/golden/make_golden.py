@@ -11,6 +11,11 @@ Fixtures (all produced by the UNMODIFIED reference compiled from its sources):
   hits_room.npz           closest/any hits of seeded random rays in the room scene
   hits_grid.npz           closest hits of seeded rays in the 1,048,576-triangle scene
   grid_film_small.npz     the sphere-grid scene at 192x108, 4 spp
+  grid_film_4096spp.npz   the sphere-grid scene (1,048,576 triangles, 2048x1024 sky with the
+                          sun) at 192x108, 4096 spp: the acceptance film of the 1080p workload's
+                          scene at reduced resolution
+
+    python tests/golden/make_golden.py --only-grid-4096   (that fixture alone)
 """
 import argparse
 import os
@@ -25,7 +30,7 @@ sys.path.insert(0, os.path.join(ROOT, "cpu-renderer_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import refimpl  # noqa: E402
 import workloads  # noqa: E402
-from crgpu import ray_dtype  # noqa: E402
+from cr_types import ray_dtype  # noqa: E402
 
 
 def random_rays(n, lo, hi, seed, y_scale=1.0, y_offset=0.0):
@@ -50,12 +55,28 @@ def grid_rays():
     return random_rays(4096, -11.0, 11.0, seed=102, y_scale=0.05, y_offset=0.5)
 
 
+def grid_4096(threads):
+    g = workloads.sphere_grid_scene(width=192, height=108, samples=4096)
+    gs = refimpl.RefScene(g["triangles"], g["materials"]).build_bvh()
+    genv = refimpl.RefEnvironment(image=g["env_image"])
+    gopt = g["options"]
+    gopt.threads = threads
+    t0 = time.time()
+    film, _ = gs.render(g["camera"], gopt, genv)
+    print(f"sphere grid 192x108 x 4096 spp: {time.time() - t0:.1f} s on {threads} threads")
+    np.savez_compressed(os.path.join(HERE, "grid_film_4096spp.npz"), film=film)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--room-spp", type=int, default=4096)
     ap.add_argument("--skip-room-4096", action="store_true")
+    ap.add_argument("--only-grid-4096", action="store_true")
     a = ap.parse_args()
     threads = os.cpu_count()
+    if a.only_grid_4096:
+        grid_4096(threads)
+        return
     sc = workloads.room_scene()
     rs = refimpl.RefScene(sc["triangles"], sc["materials"]).build_bvh()
     env = refimpl.RefEnvironment()

@@ -1,0 +1,197 @@
+"""Parity on the 1,048,576-triangle sphere-grid scene the 1920x1080 x 64 spp bench renders
+(2048x1024 log-normal sky with a 5e4 sun disk), and checks of the alias-table environment
+sampler.
+
+* Every ray of a real render — closest-hit rays at every bounce and the shadow rays — is
+  recorded by the render itself (cr_gpu_render_trace_dump) and handed to the reference's
+  Bvh::intersect (geometry.cpp:554-639) with the same ignoreTriangle: found flags, triangle,
+  t, u and v bit for bit, for both traversals (the family of test_geometry.cpp:533-570, on
+  the rays trace() produces, render.cpp:241 and 284-285).
+* Per-sample radiance of the GPU render against the CPU restatement's (whose films equal the
+  reference's byte for byte, tests/test_oracle.py).
+* The film at 4096 spp against the reference's own render (committed fixture made by
+  tests/golden/make_golden.py): relMSE <= 1e-4.
+* The alias table: its texel histogram against the CDF's per-texel probabilities, its
+  densities against the CDF's, its film against the CDF sampler's film, and the draws the
+  NEE-null shading class consumes for a light sample it skips.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import workloads
+from conftest import golden
+from crgpu import Tuning
+
+pytestmark = pytest.mark.gpu
+
+
+def tuning(**kw):
+    t = Tuning()
+    for k, v in kw.items():
+        setattr(t, k, v)
+    return t
+
+
+@pytest.fixture(scope="module")
+def grid(crgpu):
+    """The bench scene at 320x180 x 6 spp (about 1.6 M traced rays)."""
+    sc = workloads.sphere_grid_scene(width=320, height=180, samples=6)
+    tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
+    g = crgpu.GpuScene(tris, sc["materials"], env=crgpu.env_desc(image=sc["env_image"]))
+    yield sc, tris, g
+    g.close()
+
+
+@pytest.mark.parametrize("exact", [0, 1])
+def test_render_rays_bit_exact_against_reference(crgpu, ref, gpu, grid, exact):
+    sc, _, g = grid
+    n, rec = g.trace_dump(sc["camera"], sc["options"], 3_000_000, tuning=tuning(exact_traversal=exact))
+    assert n == len(rec) >= 1_000_000, n
+    rs = ref.RefScene(sc["triangles"], sc["materials"]).build_bvh()
+    closest, shadow = rec[rec["kind"] == 0], rec[rec["kind"] == 1]
+    assert len(shadow) >= 100_000
+    depths = set(np.unique(closest["depth"]).tolist())
+    assert set(range(16)) <= depths, sorted(depths)  # bounces 0-15 all traced
+    f, h = rs.intersect_rays(closest["ray"], closest["ignore"], any_hit=False)
+    mine = closest["found"].astype(bool)
+    bad = np.where(mine != f)[0]
+    assert len(bad) == 0, f"found differs on {len(bad)} of {len(closest)} closest-hit rays, e.g. {bad[:5]}"
+    for k in ("triangle", "t", "u", "v"):
+        diff = np.where(f & (closest["hit"][k] != h[k]))[0]
+        assert len(diff) == 0, f"{k} differs on {len(diff)} rays, e.g. {diff[:5]}"
+    fa, _ = rs.intersect_rays(shadow["ray"], shadow["ignore"], any_hit=True)
+    bad = np.where(shadow["found"].astype(bool) != fa)[0]
+    assert len(bad) == 0, f"any-hit differs on {len(bad)} of {len(shadow)} shadow rays"
+    print(f"exact={exact}: {len(closest)} closest-hit rays (depths {min(depths)}-{max(depths)}), "
+          f"{len(shadow)} shadow rays, all identical to Bvh::intersect")
+
+
+def test_grid_per_sample_streams_against_restatement(crgpu, gpu):
+    """Every camera sample's radiance against the CPU restatement's on the same streams."""
+    import oracle
+    sc = workloads.sphere_grid_scene(width=64, height=36, samples=8)
+    tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
+    env = crgpu.env_desc(image=sc["env_image"])
+    g = crgpu.GpuScene(tris, sc["materials"], env=env)
+    cam, opt = sc["camera"], sc["options"]
+    _, mine = g.render_resident(cam, opt, per_sample=True)
+    film = g.film(opt.width, opt.height)
+    bvh = crgpu.build_bvh(tris)
+    ofilm, theirs, _ = oracle.render_arrays(tris, sc["materials"], bvh, cam, opt, env=env, per_sample=True)
+    same = np.all(mine == theirs, axis=-1)
+    frac = float(same.mean())
+    print(f"per-sample radiance bit-identical for {frac:.4f} of {same.size} samples")
+    assert frac > 0.9, frac
+    # the film is the ordered FP64 sum of the samples, and close to the restatement's film
+    acc = mine.astype(np.float64).sum(axis=0)
+    assert np.array_equal((acc / opt.samples).astype(np.float32), film)
+    assert crgpu.rel_mse(film, ofilm) < 1e-4
+    g.close()
+
+
+def test_grid_4096spp_relmse_against_reference_render(crgpu, gpu):
+    """Acceptance on the bench scene: 192x108 at 4096 spp against the reference's render of
+    the same scene, sky and streams (committed fixture), relMSE <= 1e-4."""
+    gold = golden("grid_film_4096spp.npz")
+    assert gold is not None
+    sc = workloads.sphere_grid_scene(width=192, height=108, samples=4096)
+    tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
+    g = crgpu.GpuScene(tris, sc["materials"], env=crgpu.env_desc(image=sc["env_image"]))
+    film, st = g.render(sc["camera"], sc["options"])
+    r, l1 = crgpu.rel_mse(film, gold["film"]), crgpu.relative_l1(film, gold["film"])
+    print(f"192x108 x 4096 spp: relMSE {r:.3e}, relative L1 {l1:.3e}, {st['device_ms']:.0f} ms on the device")
+    assert r <= 1e-4, r
+    g.close()
+
+
+# ---- alias-table environment sampling ------------------------------------------------------------
+
+def _sky_scene(crgpu, width=1024, height=512):
+    sky = workloads.sky_image(width=width, height=height)
+    t = crgpu.new_triangles(1)
+    t["v"]["position"][0] = [[100, 100, 100], [101, 100, 100], [100, 101, 100]]
+    m = crgpu.new_materials(1)
+    tris, _ = crgpu.finalize(t, m)
+    env = crgpu.env_desc(image=sky)
+    return crgpu.GpuScene(tris, m, env=env), env, sky
+
+
+def _cdf_probabilities(crgpu, env, n):
+    cdf = np.zeros(n, np.float64)
+    ws = np.zeros(2, np.float64)
+    crgpu.check(crgpu.lib.cr_environment_tables(ctypes.byref(env), cdf.ctypes.data, ws.ctypes.data))
+    return np.diff(cdf, prepend=0.0) / ws[0]
+
+
+def _solid_angles(width, height):
+    pi = np.float64(np.float32(np.pi))  # the reference's float pi, widened
+    y = np.arange(height, dtype=np.float64)
+    om = (2 * pi / width) * (np.cos(pi * y / height) - np.cos(pi * (y + 1) / height))
+    return np.repeat(om, width)
+
+
+@pytest.mark.parametrize("alias", [False, True])
+def test_environment_sampler_texel_histogram(crgpu, gpu, alias):
+    """2^25 samples of the 1024x512 sky with its sun: the texel histogram against the CDF's
+    per-texel probabilities (chi-square over 4096 bands of 128 texels, and the sun's texels
+    alone), and the reported densities against the CDF's."""
+    W, H = 1024, 512
+    g, env, _ = _sky_scene(crgpu, W, H)
+    n = W * H
+    p = _cdf_probabilities(crgpu, env, n)
+    N = 1 << 25
+    tex, dens = g.environment_sample(N, alias=alias, seed=11)
+    assert tex.max() < n
+    # densities: the CDF's own (CDF mode), or the alias sampler's realised probabilities,
+    # equal to the CDF's wherever a texel carries non-negligible probability
+    om = _solid_angles(W, H)
+    got = dens.astype(np.float64) * om[tex]
+    big = p[tex] * n > 1e-3
+    rel = np.abs(got[big] / p[tex][big] - 1)
+    assert rel.max() < 2e-6, rel.max()
+    counts = np.bincount(tex, minlength=n).astype(np.float64)
+    obs, exp = counts.reshape(-1, 128).sum(1), N * p.reshape(-1, 128).sum(1)
+    keep = exp >= 20
+    chi2, dof = float(((obs[keep] - exp[keep]) ** 2 / exp[keep]).sum()), int(keep.sum()) - 1
+    print(f"alias={alias}: chi-square {chi2:.0f} on {dof} degrees of freedom")
+    assert chi2 < dof + 6 * np.sqrt(2 * dof), (chi2, dof)
+    sun = p * n > 100  # the sun disk's texels
+    assert sun.any()
+    ps, cs = p[sun].sum(), counts[sun].sum()
+    assert abs(cs - N * ps) < 5 * np.sqrt(N * ps * (1 - ps)) + 1, (cs, N * ps)
+    g.close()
+
+
+def test_alias_film_is_unbiased_against_cdf_film(crgpu, gpu):
+    """The alias sampler draws other streams, so films differ by noise only: the alias film
+    sits within the CDF sampler's own seed-to-seed noise of the CDF film."""
+    sc = workloads.sphere_grid_scene(width=64, height=36, samples=2048)
+    tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
+    g = crgpu.GpuScene(tris, sc["materials"], env=crgpu.env_desc(image=sc["env_image"]))
+    cam, opt = sc["camera"], sc["options"]
+    cdf, _ = g.render(cam, opt)
+    ali, _ = g.render(cam, opt, tuning=tuning(env_alias=1))
+    opt.seed = 7
+    cdf2, _ = g.render(cam, opt)
+    noise = crgpu.rel_mse(cdf2, cdf)
+    err = crgpu.rel_mse(ali, cdf)
+    m = [float(f.astype(np.float64).mean()) for f in (cdf, ali, cdf2)]
+    print(f"relMSE alias vs cdf {err:.3e}, cdf seed 7 vs 42 {noise:.3e}; film means {m}")
+    assert not np.array_equal(ali, cdf)
+    assert err < 3 * noise, (err, noise)
+    assert abs(m[1] / m[0] - 1) < 3 * abs(m[2] / m[0] - 1) + 0.01
+    g.close()
+
+
+@pytest.mark.parametrize("alias", [0, 1])
+def test_nee_null_class_consumes_the_light_samples_draws(crgpu, gpu, grid, alias):
+    """Hits on smooth dielectrics (the NEE-null class) skip the light sample's arithmetic but
+    must advance the stream by the same draws: the film equals the one every hit shades
+    through the generic kernel, with either environment sampler."""
+    sc, _, g = grid
+    opt = crgpu.Options.make(width=160, height=90, samples=4, bounces=16, seed=42)
+    a, _ = g.render(sc["camera"], opt, tuning=tuning(env_alias=alias))
+    b, _ = g.render(sc["camera"], opt, tuning=tuning(env_alias=alias, generic_shading=1))
+    assert a.tobytes() == b.tobytes()

@@ -36,9 +36,13 @@ def test_noalloc_render_matches_cr_gpu_render_twice(crgpu, gpu):
     cam, opt = sc["camera"], sc["options"]
     expected, st = g.render(cam, opt)
     for call in range(2):
+        before = crgpu.allocation_count()
         status, film, stats = render_noalloc(crgpu, g, cam, opt)
         assert status == 0, crgpu.last_error()
+        # the property the entry point exists for: the library requested no memory block
+        assert crgpu.allocation_count() == before, f"call {call} allocated"
         assert stats["camera_samples"] == st["camera_samples"]
+        assert stats["device_ms"] > 0
         assert np.array_equal(film, expected), f"call {call}: relMSE {crgpu.rel_mse(film, expected)}"
 
 
@@ -49,8 +53,10 @@ def test_noalloc_render_with_environment_and_several_chunks(crgpu, gpu):
     g = crgpu.GpuScene(tris, sc["materials"], env=crgpu.env_desc(image=sc["env_image"]))
     expected, _ = g.render(sc["camera"], sc["options"])
     for call in range(2):
+        before = crgpu.allocation_count()
         status, film, stats = render_noalloc(crgpu, g, sc["camera"], sc["options"])
         assert status == 0, crgpu.last_error()
+        assert crgpu.allocation_count() == before, f"call {call} allocated"
         assert stats["chunks"] == 2
         assert np.array_equal(film, expected), f"call {call}"
 

@@ -19,16 +19,37 @@
 
 namespace crg {
 
-// A chunk of consecutive sample ids [c0, c1); out[] holds their radiance at id - c0.
+// A chunk of consecutive sample ids [c0, c1) (id = sample * pixels + pixel); out[] holds the
+// radiance of id at j = id - c0, its position in the chunk. Where the chunk is whole samples
+// per pixel (spp > 0: samples [s0, s0 + spp) of every pixel) its ids are issued pixel-major:
+// position j starts sample s0 + j % spp of pixel j / spp, so the consecutive path slots that
+// form a warp start samples of one pixel and trace nearly the same rays for longer (a smooth
+// dielectric or a mirror sends them the same way). Either order, each pixel's samples are
+// summed in sample order, so the film does not depend on it.
 struct Chunk {
     uint64_t c0, c1, pixels;
+    uint32_t spp = 0, s0 = 0;  // spp 0: sample-major positions
 };
 
-// Where a path's sample radiance goes: out[base + sample * pixels + pixel].
+// Where a path's sample radiance goes: out[base + sample * sampleStride + pixel * pixelStride].
 struct OutRef {
-    uint64_t base, pixels;
+    uint64_t base, sampleStride, pixelStride;
 };
-CR_D OutRef outOf(const Chunk& C) { return OutRef{0ull - C.c0, C.pixels}; }
+CR_D OutRef outOf(const Chunk& C) {
+    if (C.spp) return OutRef{0ull - C.s0, 1, C.spp};
+    return OutRef{0ull - C.c0, C.pixels, 1};
+}
+// The pixel and sample that position j of the chunk starts.
+CR_D void chunkSample(const Chunk& C, uint64_t j, uint32_t& pixel, uint32_t& sample) {
+    if (C.spp) {
+        pixel = static_cast<uint32_t>(j / C.spp);
+        sample = C.s0 + static_cast<uint32_t>(j % C.spp);
+    } else {
+        const uint64_t id = C.c0 + j;
+        pixel = static_cast<uint32_t>(id % C.pixels);
+        sample = static_cast<uint32_t>(id / C.pixels);
+    }
+}
 
 // ---- multi-job pool ----------------------------------------------------------------------------
 // In the multi-job engine the paths of many renders (jobs: scene, camera, options) share one
@@ -135,11 +156,28 @@ CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     return true;
 }
 
+// Path state is read once per launch and is far larger than L2: CR_HINT_STREAM loads it as
+// streaming data (evict first), so it does not displace the scene's records.
+template <class T> CR_D T ld_path(const T* p) {
+#ifdef CR_HINT_STREAM
+    return __ldcs(p);
+#else
+    return *p;
+#endif
+}
+template <class T> CR_D void st_path(T* p, T v) {
+#ifdef CR_HINT_STREAM
+    __stcs(p, v);
+#else
+    *p = v;
+#endif
+}
+
 CR_D TRay loadRay(const PathSoA& st, uint32_t path, uint32_t flags) {
-    const float4 o = st.ray_o[path], d = st.ray_d[path];
+    const float4 o = ld_path(st.ray_o + path), d = ld_path(st.ray_d + path);
     TRay r;
     r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w;
-    r.olow = (flags & kPathPrecise) ? v3(st.ray_lo[path]) : V3{};
+    r.olow = (flags & kPathPrecise) ? v3(ld_path(st.ray_lo + path)) : V3{};
     return r;
 }
 
@@ -150,7 +188,7 @@ CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, 
         raise(E, P, pixel, sample, kErrNonFiniteRadiance);
         R = V3{};
     }
-    st.out[O.base + static_cast<uint64_t>(sample) * O.pixels + pixel] = f4(R, 0);
+    st.out[O.base + static_cast<uint64_t>(sample) * O.sampleStride + static_cast<uint64_t>(pixel) * O.pixelStride] = f4(R, 0);
     if (st.guide.count) guideFinish(st.guide, path, R);
 }
 
@@ -427,7 +465,7 @@ CR_D bool shadowFinish(const RenderParams& P, const OutRef& O, const PathSoA& st
 // What follows a path's closest-hit query: the hit is recorded and its shading class returned.
 CR_D int closestFinish(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
                        bool found, const HitRec& h, int err) {
-    st.hit_tri[path] = found ? h.tri : kNoTriangle;
+    st_path(st.hit_tri + path, found ? h.tri : kNoTriangle);
     if (st.guide.hitT) st.guide.hitT[path] = found ? static_cast<float>(h.t) : 0.0f;
     if (err) raise(E, P, st.pixel[path], st.sample[path], err);
     if (!found) return kShadeMiss;
@@ -457,7 +495,8 @@ CR_D void dumpRay(const TraceDump& D, const TRay& r, uint32_t ignore, uint32_t k
 template <bool COUNT = false, bool NOALPHA = false>
 CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
                     const ErrSink& E, unsigned long long* stats = nullptr) {
-    const float4 o = st.sh_o[path], d = st.sh_d[path], lo = st.sh_lo[path], c = st.sh_c[path];
+    const float4 o = ld_path(st.sh_o + path), d = ld_path(st.sh_d + path), lo = ld_path(st.sh_lo + path),
+                 c = ld_path(st.sh_c + path);
     TRay r;
     r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w; r.olow = v3(lo);
     HitRec h;
@@ -477,14 +516,14 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
 template <bool COUNT, bool NOALPHA = false>
 CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
                     unsigned long long* stats) {
-    const uint32_t flags = st.flags[path];
+    const uint32_t flags = ld_path(st.flags + path);
     const TRay r = loadRay(st, path, flags);
     HitRec h;
     h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
     int err = 0;
     VisitCount vc;
-    const bool found = intersect<false, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), st.prev_tri[path], P.exact_traversal != 0,
-                                               h, err, &vc);
+    const bool found = intersect<false, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), ld_path(st.prev_tri + path),
+                                               P.exact_traversal != 0, h, err, &vc);
     if (COUNT) {
         atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
         atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
@@ -508,7 +547,7 @@ CR_D PathJob pathJob(const JobTable& J, uint32_t path) {
     PathJob pj;
     pj.S = J.scenes + R.job;
     pj.P = J.params + R.job;
-    pj.O = OutRef{R.outBase - R.c0, R.pixels};
+    pj.O = OutRef{R.outBase - R.c0, R.pixels, 1};
     pj.E = ErrSink{J.errKeys + R.job, nullptr};
     pj.retries = J.retries + R.job;
     pj.r = r;
@@ -568,7 +607,8 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
             const uint64_t id = first + __popc(mask & ((1u << lane) - 1u));
             bool live = false;
             if (have && id < C.c1) {
-                const uint32_t pixel = static_cast<uint32_t>(id % C.pixels), sample = static_cast<uint32_t>(id / C.pixels);
+                uint32_t pixel, sample;
+                chunkSample(C, id - C.c0, pixel, sample);
                 live = initPath(S, P, st, slot, pixel, sample, false, E);
                 if (!live) st.out[id - C.c0] = make_float4(0, 0, 0, 0);
             }
@@ -689,6 +729,19 @@ __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
 
 // render.cpp:390-413: each pixel adds the chunk's samples in index order.
 static __global__ void k_accumulate(const float4* out, Chunk C, double* acc) {
+    if (C.spp) {  // pixel-major chunk: a pixel's samples are consecutive
+        for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < C.pixels;
+             p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+            double r = acc[3 * p], g = acc[3 * p + 1], b = acc[3 * p + 2];
+            const float4* o = out + p * C.spp;
+            for (uint32_t k = 0; k < C.spp; ++k) {
+                const float4 v = o[k];
+                r += v.x; g += v.y; b += v.z;
+            }
+            acc[3 * p] = r; acc[3 * p + 1] = g; acc[3 * p + 2] = b;
+        }
+        return;
+    }
     for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < C.pixels;
          p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t sBegin = C.c0 > p ? (C.c0 - p + C.pixels - 1) / C.pixels : 0;
@@ -702,10 +755,12 @@ static __global__ void k_accumulate(const float4* out, Chunk C, double* acc) {
     }
 }
 // Copies the chunk's radiance as packed RGB (sample-major) for stream-level comparisons.
-static __global__ void k_pack_samples(const float4* out, uint64_t n, float* dst) {
+static __global__ void k_pack_samples(const float4* out, Chunk C, float* dst) {
+    const uint64_t n = C.c1 - C.c0;
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const float4 o = out[i];
-        dst[3 * i] = o.x; dst[3 * i + 1] = o.y; dst[3 * i + 2] = o.z;
+        const uint64_t d = C.spp ? (i % C.spp) * C.pixels + i / C.spp : i;
+        dst[3 * d] = o.x; dst[3 * d + 1] = o.y; dst[3 * d + 2] = o.z;
     }
 }
 // render.cpp:415

@@ -634,6 +634,9 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                         : frames.format == CR_ENCODE_RGBE ? 4 * pixels
                         : crh::hdr_header(o.width, o.height).size() + static_cast<uint64_t>(o.height) * (4 + 8ull * o.width + 8));
     }
+    // Chunks of whole samples per pixel (where one fits the pool) issue their ids pixel-major
+    // (see Chunk): the default chunk is the most whole samples of every pixel the pool holds.
+    if (!tuning.chunk_log2 && !frames.every && !guide && chunk >= pixels) chunk = chunk / pixels * pixels;
     // a pool never needs more slots than one chunk has samples
     pool = std::min<uint64_t>(pool, chunk);
     pool = (pool + 127) / 128 * 128;
@@ -728,7 +731,11 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
             st.guide.records = nullptr;
             st.guide.record = 0;
         }
-        const Chunk C{c0, std::min<uint64_t>(total, c0 + step), pixels};
+        Chunk C{c0, std::min<uint64_t>(total, c0 + step), pixels};
+        if (c0 % pixels == 0 && (C.c1 - c0) % pixels == 0) {  // whole samples: pixel-major
+            C.spp = static_cast<uint32_t>((C.c1 - c0) / pixels);
+            C.s0 = static_cast<uint32_t>(c0 / pixels);
+        }
         ++chunks;
         // the chunk's ids are issued from c0
         CR_CUDA(cudaMemsetAsync(W.counts, 0, kCountWords * sizeof(uint32_t), s));
@@ -865,7 +872,7 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         }
         if (perSample) {
             const uint64_t n = C.c1 - C.c0;
-            k_pack_samples<<<W.gridSmall, 128, 0, s>>>(st.out, n, W.packed);
+            k_pack_samples<<<W.gridSmall, 128, 0, s>>>(st.out, C, W.packed);
             CR_CUDA(cudaMemcpyAsync(perSample + 3 * C.c0, W.packed, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
             CR_CUDA(cudaStreamSynchronize(s));
         }

@@ -39,6 +39,11 @@ CR_D OutRef outOf(const Chunk& C) {
     if (C.spp) return OutRef{0ull - C.s0, 1, C.spp};
     return OutRef{0ull - C.c0, C.pixels, 1};
 }
+// out[] index of a pixel's sample
+CR_D uint64_t outIndex(const OutRef& O, uint32_t pixel, uint32_t sample) {
+    return O.base + static_cast<uint64_t>(sample) * O.sampleStride + static_cast<uint64_t>(pixel) * O.pixelStride;
+}
+
 // The pixel and sample that position j of the chunk starts.
 CR_D void chunkSample(const Chunk& C, uint64_t j, uint32_t& pixel, uint32_t& sample) {
     if (C.spp) {
@@ -156,28 +161,11 @@ CR_D bool initPath(const DevScene& S, const RenderParams& P, const PathSoA& st, 
     return true;
 }
 
-// Path state is read once per launch and is far larger than L2: CR_HINT_STREAM loads it as
-// streaming data (evict first), so it does not displace the scene's records.
-template <class T> CR_D T ld_path(const T* p) {
-#ifdef CR_HINT_STREAM
-    return __ldcs(p);
-#else
-    return *p;
-#endif
-}
-template <class T> CR_D void st_path(T* p, T v) {
-#ifdef CR_HINT_STREAM
-    __stcs(p, v);
-#else
-    *p = v;
-#endif
-}
-
 CR_D TRay loadRay(const PathSoA& st, uint32_t path, uint32_t flags) {
-    const float4 o = ld_path(st.ray_o + path), d = ld_path(st.ray_d + path);
+    const float4 o = st.ray_o[path], d = st.ray_d[path];
     TRay r;
     r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w;
-    r.olow = (flags & kPathPrecise) ? v3(ld_path(st.ray_lo + path)) : V3{};
+    r.olow = (flags & kPathPrecise) ? v3(st.ray_lo[path]) : V3{};
     return r;
 }
 
@@ -188,7 +176,7 @@ CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, 
         raise(E, P, pixel, sample, kErrNonFiniteRadiance);
         R = V3{};
     }
-    st.out[O.base + static_cast<uint64_t>(sample) * O.sampleStride + static_cast<uint64_t>(pixel) * O.pixelStride] = f4(R, 0);
+    st.out[outIndex(O, pixel, sample)] = f4(R, 0);
     if (st.guide.count) guideFinish(st.guide, path, R);
 }
 
@@ -465,7 +453,7 @@ CR_D bool shadowFinish(const RenderParams& P, const OutRef& O, const PathSoA& st
 // What follows a path's closest-hit query: the hit is recorded and its shading class returned.
 CR_D int closestFinish(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
                        bool found, const HitRec& h, int err) {
-    st_path(st.hit_tri + path, found ? h.tri : kNoTriangle);
+    st.hit_tri[path] = found ? h.tri : kNoTriangle;
     if (st.guide.hitT) st.guide.hitT[path] = found ? static_cast<float>(h.t) : 0.0f;
     if (err) raise(E, P, st.pixel[path], st.sample[path], err);
     if (!found) return kShadeMiss;
@@ -495,8 +483,7 @@ CR_D void dumpRay(const TraceDump& D, const TRay& r, uint32_t ignore, uint32_t k
 template <bool COUNT = false, bool NOALPHA = false>
 CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
                     const ErrSink& E, unsigned long long* stats = nullptr) {
-    const float4 o = ld_path(st.sh_o + path), d = ld_path(st.sh_d + path), lo = ld_path(st.sh_lo + path),
-                 c = ld_path(st.sh_c + path);
+    const float4 o = st.sh_o[path], d = st.sh_d[path], lo = st.sh_lo[path], c = st.sh_c[path];
     TRay r;
     r.o = v3(o); r.tmin = o.w; r.d = v3(d); r.tmax = d.w; r.olow = v3(lo);
     HitRec h;
@@ -516,13 +503,13 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
 template <bool COUNT, bool NOALPHA = false>
 CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st, uint32_t path, const ErrSink& E,
                     unsigned long long* stats) {
-    const uint32_t flags = ld_path(st.flags + path);
+    const uint32_t flags = st.flags[path];
     const TRay r = loadRay(st, path, flags);
     HitRec h;
     h.t = kInf; h.u = 0; h.v = 0; h.tri = 0;
     int err = 0;
     VisitCount vc;
-    const bool found = intersect<false, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), ld_path(st.prev_tri + path),
+    const bool found = intersect<false, COUNT, NOALPHA>(S, r, static_cast<double>(kInf), st.prev_tri[path],
                                                P.exact_traversal != 0, h, err, &vc);
     if (COUNT) {
         atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));

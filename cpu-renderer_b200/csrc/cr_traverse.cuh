@@ -96,47 +96,10 @@ CR_D bool accepts(const DevScene& S, uint32_t tri, uint32_t flags, V3 dir, doubl
     return true;
 }
 
-// Loads of the scene's node and triangle records. CR_HINT_NODES asks the caches to keep them
-// (L1 and L2 evict-last) ahead of the path state that streams through every launch.
-CR_D float4 ld_scene(const float4* p) {
-#ifdef CR_HINT_NODES
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    float4 v;
-    asm("ld.global.nc.L1::evict_last.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
-    return v;
-#else
-    return __ldg(p);
-#endif
-}
-CR_D uint4 ld_scene(const uint4* p) {
-#ifdef CR_HINT_NODES
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    uint4 v;
-    asm("ld.global.nc.L1::evict_last.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(pol));
-    return v;
-#else
-    return __ldg(p);
-#endif
-}
-
 CR_D void load_pair(const NodePair* pairs, uint32_t p, float4& a, float4& b, float4& c, uint4& d) {
     const float4* q = reinterpret_cast<const float4*>(pairs + p);
-    a = ld_scene(q); b = ld_scene(q + 1); c = ld_scene(q + 2);
-    d = ld_scene(reinterpret_cast<const uint4*>(q + 3));
-}
-
-// A node pair or leaf the traversal will probably visit later (the far child it pushes):
-// CR_PREFETCH_FAR starts bringing it into L1 now.
-CR_D void prefetch_child(const DevScene& S, uint32_t ref, uint32_t cnt) {
-#ifdef CR_PREFETCH_FAR
-    const void* p = cnt ? static_cast<const void*>(S.tri_pos + 3 * static_cast<uint64_t>(ref))
-                        : static_cast<const void*>(S.pairs + ref);
-    asm volatile("prefetch.global.L1 [%0];" : : "l"(p));
-#endif
+    a = __ldg(q); b = __ldg(q + 1); c = __ldg(q + 2);
+    d = __ldg(reinterpret_cast<const uint4*>(q + 3));
 }
 
 // ---- exact traversal (geometry.cpp:554-639) ------------------------------------------------
@@ -335,82 +298,6 @@ CR_D bool tri_reject_fast(const FastSetup& F, float4 p0, float4 p1, float4 p2) {
     return (w0 < -dw || w1 < -dw || w2 < -dw) && (w0 > dw || w1 > dw || w2 > dw);
 }
 
-// The FP32 triangle test of the deferred traversal: the edge functions and their error bound
-// as tri_reject_fast computes them, then what they prove about the reference's FP64 test.
-//   kind 0: the reference rejects the triangle (mixed signs beyond the bound);
-//   kind 1: it may accept it; [tlo, thi] brackets its t when the determinant is well away from
-//           zero (else tlo = -inf, thi = +inf);
-//   kind 2: the edge functions certainly share a sign (the reference sees an inside point with
-//           a non-zero determinant) and [tlo, thi] brackets its t.
-// Bounds (forward error analysis as for tri_reject_fast; u = 2^-24): |dw| bounds each edge
-// function's error; the determinant w0+w1+w2 then errs by at most 3|dw| + 3u(|w0|+|w1|+|w2|),
-// the numerator sum(w_i z_i) by 3|dw| max|z| + 4u (|w0|+|w1|+|w2|) max|z|, and the quotient
-// t = numerator * (1/dz) / det adds a few roundings of t itself. The bracket doubles the
-// first-order sum, which covers the second-order terms once |det| >= 64 |dw|, and the FP64
-// arithmetic of the reference sits ~2^-29 inside every FP32 bound.
-struct TriFast {
-    int kind;
-    float tlo, thi;
-};
-CR_D TriFast tri_test_fast(const FastSetup& F, float4 p0, float4 p1, float4 p2) {
-    const float ox = F.o[F.kx], oy = F.o[F.ky], oz = F.o[F.kz];
-    const float axk = pick(p0, F.kx) - ox, ayk = pick(p0, F.ky) - oy, azk = pick(p0, F.kz) - oz;
-    const float bxk = pick(p1, F.kx) - ox, byk = pick(p1, F.ky) - oy, bzk = pick(p1, F.kz) - oz;
-    const float cxk = pick(p2, F.kx) - ox, cyk = pick(p2, F.ky) - oy, czk = pick(p2, F.kz) - oz;
-    const float ax = __fmaf_rn(-F.Sx, azk, axk), ay = __fmaf_rn(-F.Sy, azk, ayk);
-    const float bx = __fmaf_rn(-F.Sx, bzk, bxk), by = __fmaf_rn(-F.Sy, bzk, byk);
-    const float cx = __fmaf_rn(-F.Sx, czk, cxk), cy = __fmaf_rn(-F.Sy, czk, cyk);
-    const float w0 = __fmaf_rn(cx, by, -(cy * bx));
-    const float w1 = __fmaf_rn(ax, cy, -(ay * cx));
-    const float w2 = __fmaf_rn(bx, ay, -(by * ax));
-    const float mz = fmaxf(fmaxf(fabsf(azk), fabsf(bzk)), fabsf(czk));
-    const float mxk = fmaxf(fmaxf(fabsf(axk), fabsf(bxk)), fabsf(cxk));
-    const float myk = fmaxf(fmaxf(fabsf(ayk), fabsf(byk)), fabsf(cyk));
-    const float mx = fmaxf(fmaxf(fabsf(ax), fabsf(bx)), fabsf(cx));
-    const float my = fmaxf(fmaxf(fabsf(ay), fabsf(by)), fabsf(cy));
-    constexpr float g = 6e-7f;  // twice gamma(5) for u = 2^-24
-    const float dx = g * (mxk + mz), dy = g * (myk + mz);
-    const float dw = 4.0f * ((mx + dx) * dy + (my + dy) * dx + g * (mx + dx) * (my + dy)) + 1e-30f;
-    TriFast r;
-    r.kind = 0;
-    r.tlo = -kInf;
-    r.thi = kInf;
-    if ((w0 < -dw || w1 < -dw || w2 < -dw) && (w0 > dw || w1 > dw || w2 > dw)) return r;
-    r.kind = 1;
-    const float det = w0 + w1 + w2;
-    const float adet = fabsf(det);
-    const float W = fabsf(w0) + fabsf(w1) + fabsf(w2);
-    if (!(adet >= 64.0f * dw) || !(W < 1e30f) || !(mz < 1e30f)) return r;
-    const float sz = F.inv[F.kz];
-    const float num = __fmaf_rn(w0, azk, __fmaf_rn(w1, bzk, w2 * czk));
-    const float t = (num * sz) / det;
-    constexpr float u = 5.9604645e-08f;  // 2^-24
-    const float at = fabsf(t);
-    const float dt = 2.0f * (at * ((3.0f * dw + 3.0f * u * W) / adet + 8.0f * u) +
-                             (3.0f * dw + 4.0f * u * W) * mz * fabsf(sz) / adet) + 1e-30f;
-    if (!isfin(t) || !isfin(dt)) return r;
-    r.tlo = t - dt;
-    r.thi = t + dt;
-    const float lim = 1.001f * dw;
-    if ((w0 > lim && w1 > lim && w2 > lim) || (w0 < -lim && w1 < -lim && w2 < -lim)) r.kind = 2;
-    return r;
-}
-
-// Closest hit by the fast traversal with the FP64 decisions deferred. The node and leaf loops
-// run in FP32 only: a leaf's triangle that the FP32 test cannot reject becomes a candidate
-// (its slot and a lower bound of its t), and one that the reference certainly accepts (kind 2,
-// t certainly inside the query interval, sidedness decided by the reference's own FP64 dot)
-// lowers the bound B that culls boxes and candidates: the reference's closest hit has t <= B,
-// so nothing whose t exceeds B can be it. When the traversal ends, the surviving candidates
-// are decided by tri_exact and accepts, the reference's arithmetic, and the minimum (t, index)
-// wins, as in intersect_fast. The loops therefore carry no FP64 state. More than
-// kCandidates candidates (coplanar clutter) send the ray through intersect_exact instead.
-constexpr int kCandidates = 16;
-
-template <bool COUNT = false, bool NOALPHA = false>
-__device__ bool intersect_fast_deferred(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore,
-                                        HitRec& hit, int& err, VisitCount* vc = nullptr);
-
 // The fast traversal in the "while-while" form of Aila and Laine ("Understanding the
 // Efficiency of Ray Traversal on GPUs", HPG 2009): an inner loop walks interior nodes and
 // postpones the first leaf it reaches, continuing speculatively until every lane of the warp
@@ -457,9 +344,7 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
                 if (size >= kStackSize) { err = kErrStackOverflow; return found; }
                 const bool firstNear = n0 <= n1;
                 stRef[size] = firstNear ? d.z : d.x; stCnt[size] = firstNear ? d.w : d.y;
-                stNear[size] = firstNear ? n1 : n0;
-                prefetch_child(S, stRef[size], stCnt[size]);
-                ++size;
+                stNear[size] = firstNear ? n1 : n0; ++size;
                 ref = firstNear ? d.x : d.z; cnt = firstNear ? d.y : d.w;
             } else if (h0) { ref = d.x; cnt = d.y; }
             else if (h1) { ref = d.z; cnt = d.w; }
@@ -469,7 +354,7 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
         }
         for (; leafCnt; ++leafRef, --leafCnt) {
             const float4* q = S.tri_pos + 3 * static_cast<uint64_t>(leafRef);
-            const float4 q0 = ld_scene(q), q1 = ld_scene(q + 1), q2 = ld_scene(q + 2);
+            const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
             if (COUNT) ++vc->tris;
             const uint32_t index = __float_as_uint(q0.w);
             if (index == ignore) continue;
@@ -493,104 +378,6 @@ __device__ bool intersect_fast(const DevScene& S, const TRay& ray, double hitT, 
     return found;
 }
 
-template <bool COUNT, bool NOALPHA>
-__device__ bool intersect_fast_deferred(const DevScene& S, const TRay& ray, double hitT, uint32_t ignore,
-                                        HitRec& hit, int& err, VisitCount* vc) {
-    const double closestLimit = smin(static_cast<double>(ray.tmax), hitT);
-    const float queryLimit = smin(ray.tmax, next_up(static_cast<float>(closestLimit)));
-    if (queryLimit < ray.tmin) return false;
-    const FastSetup F = fast_setup(ray);
-    float rootNear;
-    if (!box_fast(F, S.root_lo[0], S.root_lo[1], S.root_lo[2], S.root_hi[0], S.root_hi[1], S.root_hi[2],
-                  ray.tmin, queryLimit, rootNear)) return false;
-    uint32_t stRef[kStackSize], stCnt[kStackSize];
-    float stNear[kStackSize];
-    uint32_t cSlot[kCandidates];
-    float cLo[kCandidates];
-    int nc = 0;
-    bool overflow = false;
-    float ctmax = queryLimit;  // B: no box or candidate beyond it can hold the closest hit
-    int size = 0;
-    uint32_t ref = S.root_ref, cnt = S.root_count;
-    bool haveNode = true;
-    uint32_t leafRef = 0, leafCnt = 0;
-    auto pop = [&]() -> bool {
-        while (size > 0) {
-            --size;
-            if (stNear[size] <= ctmax) { ref = stRef[size]; cnt = stCnt[size]; return true; }
-        }
-        return false;
-    };
-    for (;;) {
-        if (haveNode && cnt && !leafCnt) { leafRef = ref; leafCnt = cnt; haveNode = pop(); }
-        while (haveNode && cnt == 0) {
-            float4 a, b, c; uint4 d;
-            load_pair(S.pairs, ref, a, b, c, d);
-            if (COUNT) ++vc->pairs;
-            float n0, n1;
-            const bool h0 = box_fast(F, a.x, a.y, a.z, a.w, b.x, b.y, ray.tmin, ctmax, n0);
-            const bool h1 = box_fast(F, b.z, b.w, c.x, c.y, c.z, c.w, ray.tmin, ctmax, n1);
-            if (h0 && h1) {
-                if (size >= kStackSize) { err = kErrStackOverflow; return false; }
-                const bool firstNear = n0 <= n1;
-                stRef[size] = firstNear ? d.z : d.x; stCnt[size] = firstNear ? d.w : d.y;
-                stNear[size] = firstNear ? n1 : n0;
-                ++size;
-                ref = firstNear ? d.x : d.z; cnt = firstNear ? d.y : d.w;
-            } else if (h0) { ref = d.x; cnt = d.y; }
-            else if (h1) { ref = d.z; cnt = d.w; }
-            else haveNode = pop();
-            if (haveNode && cnt && !leafCnt) { leafRef = ref; leafCnt = cnt; haveNode = pop(); }
-            if (__all_sync(__activemask(), leafCnt != 0)) break;
-        }
-        for (; leafCnt; ++leafRef, --leafCnt) {
-            const float4* q = S.tri_pos + 3 * static_cast<uint64_t>(leafRef);
-            const float4 q0 = ld_scene(q), q1 = ld_scene(q + 1), q2 = ld_scene(q + 2);
-            if (COUNT) ++vc->tris;
-            const uint32_t index = __float_as_uint(q0.w);
-            if (index == ignore) continue;
-            const TriFast tf = tri_test_fast(F, q0, q1, q2);
-            if (tf.kind == 0 || tf.tlo > ctmax || tf.thi < ray.tmin) continue;
-            const uint32_t flags = __float_as_uint(q1.w);
-            if ((flags & kTriCull) && !accepts_cull(S, index, ray.d)) continue;  // the reference's own test
-            if (tf.kind == 2 && tf.tlo >= ray.tmin && static_cast<double>(tf.thi) <= closestLimit &&
-                (NOALPHA || !(flags & kTriAlphaMask)) && tf.thi < ctmax) {
-                ctmax = tf.thi;  // a certain hit: drop the candidates it proves too far
-                int keep = 0;
-                for (int i = 0; i < nc; ++i)
-                    if (cLo[i] <= ctmax) { cSlot[keep] = cSlot[i]; cLo[keep] = cLo[i]; ++keep; }
-                nc = keep;
-            }
-            if (nc < kCandidates) { cSlot[nc] = leafRef; cLo[nc] = tf.tlo; ++nc; }
-            else overflow = true;
-        }
-        if (!haveNode) break;
-    }
-    if (overflow) return intersect_exact<false, COUNT, NOALPHA>(S, ray, hitT, ignore, hit, err, vc);
-    if (nc == 0) return false;
-    // the reference's decisions for the candidates left: minimum (t, index) over those it accepts
-    const ExactSetup E = exact_setup(ray);
-    const double limit = smin(static_cast<double>(queryLimit), closestLimit);
-    bool found = false;
-    double bestW1 = 0, bestW2 = 0, bestDet = 1;
-    for (int i = 0; i < nc; ++i) {
-        if (cLo[i] > ctmax) continue;
-        const float4* q = S.tri_pos + 3 * static_cast<uint64_t>(cSlot[i]);
-        const float4 q0 = ld_scene(q), q1 = ld_scene(q + 1), q2 = ld_scene(q + 2);
-        const uint32_t index = __float_as_uint(q0.w);
-        double t, w1, w2, det;
-        if (!tri_exact(E, v3(q0), v3(q1), v3(q2), ray.tmin, limit, t, w1, w2, det)) continue;
-        const uint32_t flags = __float_as_uint(q1.w);
-        if (!NOALPHA && (flags & kTriAlphaMask) && !accepts_alpha(S, index, w1 / det, w2 / det)) continue;
-        if (!found || t < hit.t || (t == hit.t && index < hit.tri)) {
-            hit.t = t; hit.tri = index; hit.flags = flags; bestW1 = w1; bestW2 = w2; bestDet = det;
-            found = true;
-        }
-    }
-    if (found) { hit.u = bestW1 / bestDet; hit.v = bestW2 / bestDet; }
-    return found;
-}
-
 // Bvh::intersect entry: the reference's preconditions (geometry.cpp:555), then the traversal
 // that fits the ray.
 template <bool ANY, bool COUNT = false, bool NOALPHA = false>
@@ -598,9 +385,6 @@ __device__ bool intersect(const DevScene& S, const TRay& ray, double hitT, uint3
                           HitRec& hit, int& err, VisitCount* vc = nullptr) {
     if (!S.has_root || !validRay(ray) || isnan(hitT)) return false;
     if (forceExact || !fast_eligible(ray)) return intersect_exact<ANY, COUNT, NOALPHA>(S, ray, hitT, ignore, hit, err, vc);
-#ifdef CR_DEFERRED_EXACT
-    if constexpr (!ANY) return intersect_fast_deferred<COUNT, NOALPHA>(S, ray, hitT, ignore, hit, err, vc);
-#endif
     return intersect_fast<ANY, COUNT, NOALPHA>(S, ray, hitT, ignore, hit, err, vc);
 }
 

@@ -31,10 +31,12 @@ enum : uint32_t { kLightPunctual = 0, kLightTriangle = 1, kLightEnvironment = 2 
 // Triangle flags in tri_pos[3*slot+1].w and tri_ng[triangle].w. kTriNeeNull marks materials
 // whose BSDF value is zero for every direction (smooth, and metallic 1 or transmission 1, no
 // texture that could change that): their next-event estimation only consumes random draws.
-enum : uint32_t { kTriCull = 1u, kTriAlphaMask = 2u, kTriNeeNull = 4u };
+// kTriConductor marks rough GGX conductors (metallic exactly 1, transmission exactly 0, no
+// texture that could change either), which the conductor shading kernel takes.
+enum : uint32_t { kTriCull = 1u, kTriAlphaMask = 2u, kTriNeeNull = 4u, kTriConductor = 8u };
 
 // Shading classes, one queue each, filled by the traversal kernel.
-enum : int { kShadeMiss = 0, kShadeNeeNull = 1, kShadeGeneric = 2, kShadeClasses = 3 };
+enum : int { kShadeMiss = 0, kShadeNeeNull = 1, kShadeGeneric = 2, kShadeConductor = 3, kShadeClasses = 4 };
 
 struct DevImage { int32_t width, height; const float4* pixels; };
 
@@ -65,6 +67,8 @@ struct DevScene {
     uint32_t image_count, texture_count;
     uint32_t any_alpha_mask;
     uint32_t nee_skip;            // kTriNeeNull surfaces may skip the light-sample arithmetic
+    uint32_t conductor_class;     // kTriConductor surfaces go to the conductor shading kernel
+                                  // (set per render by the launchers that run that kernel)
     // lights (render.cpp:120-229)
     const LightEntry* light_entries;
     uint32_t light_entry_count;
@@ -169,7 +173,9 @@ struct Queues {
 // kCountTraceWork0/1: queue entries k_trace has handed out (indexed by iteration parity);
 // kCountShadeWork0 + class: the same for each k_shade instantiation.
 enum { kCountExtend0 = 0, kCountExtend1 = 1, kCountShadow0 = 2, kCountShadow1 = 3, kCountFree0 = 4, kCountFree1 = 5,
-       kCountShade0 = 6, kCountTraceWork0 = 9, kCountShadeWork0 = 11, kCountWords = 16 };
+       kCountShade0 = 6, kCountTraceWork0 = kCountShade0 + kShadeClasses, kCountShadeWork0 = kCountTraceWork0 + 2,
+       kCountWords = kCountShadeWork0 + kShadeClasses };
+static_assert(kCountWords == 16, "queue counter words");
 
 // Device error record; the host reports the one with the smallest key, which is the
 // order a single reference worker would meet them (tiles, rows, columns, samples).

@@ -184,7 +184,8 @@ CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, 
 // closest hit is known. cont: the path continues; shadow: a shadow ray was queued (a path
 // that ends with a queued shadow ray is finished by k_trace next iteration); freed: the path
 // ended and its slot can take a new sample. CLASS specialises the code: kShadeMiss holds only
-// environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeGeneric anything.
+// environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeConductor only
+// hits on kTriConductor surfaces (the BSDF without its zero lobes), kShadeGeneric anything.
 template <int CLASS, bool GUIDED = false, bool LEAN = false>
 CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
                    const ErrSink& E, unsigned long long* retries, bool& cont, bool& shadow, bool& freed) {
@@ -253,7 +254,8 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
         const LightSample light = sampleLight<LEAN>(S, s.position, rng, P.env_alias, err);
         const bool enclosedInfinite = medium >= 0 && s.thickness <= 0 && !isfin(light.distance);
         if (!enclosedInfinite && light.pdf > 0 && maxComponent(light.radiance) > 0) {
-            const BsdfEval bsdf = evaluateBsdf(s, wo, light.direction);
+            const BsdfEval bsdf = CLASS == kShadeConductor ? evaluateConductor(s, wo, light.direction)
+                                                           : evaluateBsdf(s, wo, light.direction);
             if (maxComponent(bsdf.value) > 0) {
                 bool ok = true;
                 if (precise) { sh.o = s.position; sh.d = light.direction; sh.tmin = 0; sh.tmax = kInf; sh.olow = s.positionLow; }
@@ -336,6 +338,8 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
         } else {
             smp = sampleBsdf(s, wo, rng);
         }
+    } else if constexpr (CLASS == kShadeConductor) {
+        smp = sampleConductor(s, wo, rng);  // render.cpp:302-303
     } else {
         smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
     }
@@ -457,7 +461,8 @@ CR_D int closestFinish(const DevScene& S, const RenderParams& P, const PathSoA& 
     if (st.guide.hitT) st.guide.hitT[path] = found ? static_cast<float>(h.t) : 0.0f;
     if (err) raise(E, P, st.pixel[path], st.sample[path], err);
     if (!found) return kShadeMiss;
-    return (S.nee_skip && (h.flags & kTriNeeNull)) ? kShadeNeeNull : kShadeGeneric;
+    if (S.nee_skip && (h.flags & kTriNeeNull)) return kShadeNeeNull;
+    return (S.conductor_class && (h.flags & kTriConductor)) ? kShadeConductor : kShadeGeneric;
 }
 
 // Records one traced ray and the traversal's answer (cr_gpu_render_trace_dump).

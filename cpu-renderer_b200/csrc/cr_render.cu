@@ -93,15 +93,17 @@ struct Workspace {
     unsigned long long* hostStats = nullptr;  // pinned
     int gridTrace = 0, gridShade = 0, gridShadeLight = 0, gridShadeMiss = 0, gridRegen = 0, gridSmall = 0;
     int gridShadeLean = 0, gridShadeLightLean = 0, gridShadeMissLean = 0, gridTraceNoAlpha = 0;
+    int gridShadeCond = 0, gridShadeCondLean = 0;
     std::vector<cudaEvent_t> events;
-    // two more streams for the shading launches that run beside the generic one
-    cudaStream_t side[2] = {nullptr, nullptr};
-    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    // more streams for the shading launches that run beside the generic one
+    static constexpr int kSide = 3;
+    cudaStream_t side[kSide] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[kSide] = {nullptr, nullptr, nullptr};
 
     void ensureSideStreams() {
         if (side[0]) return;
         CR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < kSide; ++k) {
             CR_CUDA(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
             CR_CUDA(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming));
         }
@@ -419,6 +421,9 @@ void uploadScene(cr_gpu_scene& g, const cr_scene_desc& d, const cr_environment_d
             if (m.roughness <= 0.001f && m.metallic_roughness_texture.texture < 0 &&
                 (m.metallic == 1.0f || (m.transmission == 1.0f && m.transmission_texture.texture < 0)))
                 f |= kTriNeeNull;
+            else if (m.metallic == 1.0f && m.transmission == 0.0f && m.metallic_roughness_texture.texture < 0 &&
+                     m.transmission_texture.texture < 0)
+                f |= kTriConductor;  // a rough GGX conductor: its BSDF has no diffuse or transmission lobe
             const bool textured = m.base_color_texture.texture >= 0 || m.metallic_roughness_texture.texture >= 0 ||
                                   m.normal_texture.texture >= 0 || m.emissive_texture.texture >= 0 ||
                                   m.transmission_texture.texture >= 0;
@@ -694,6 +699,8 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
         W.gridShadeLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric, false, false, true>), 128, g.device);
         W.gridShadeLightLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull, false, false, true>), 128, g.device);
         W.gridShadeMissLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss, false, false, true>), 128, g.device);
+        W.gridShadeCond = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeConductor>), 128, g.device);
+        W.gridShadeCondLean = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeConductor, false, false, true>), 128, g.device);
         W.gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen<false>), 128, g.device);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
@@ -706,6 +713,8 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     DevScene dev = g.dev;
     if (tuning.env_alias && g.dev.env_has_image) dev.env_pdf = g.aliasPdf;
     if (tuning.generic_shading) dev.nee_skip = 0;
+    // rough conductors take their own kernel (guided renders shade them in the guided generic one)
+    dev.conductor_class = !guide && !tuning.generic_shading ? 1u : 0u;
     CR_CUDA(cudaMemsetAsync(g.acc, 0, 3 * pixels * sizeof(double), s));
     CR_CUDA(cudaMemsetAsync(W.stats, 0, kStatWords * sizeof(unsigned long long), s));
     const unsigned long long noError = ~0ull;
@@ -779,28 +788,34 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
                 // fills the device while the others drain.
                 if (!timePhases && !guide) {
                     CR_CUDA(cudaEventRecord(W.fork, s));
-                    for (int k = 0; k < 2; ++k) CR_CUDA(cudaStreamWaitEvent(W.side[k], W.fork, 0));
+                    for (int k = 0; k < Workspace::kSide; ++k) CR_CUDA(cudaStreamWaitEvent(W.side[k], W.fork, 0));
                     if (lean) {
                         k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, W.side[0]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                         k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, W.side[1]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeConductor, false, false, true><<<cap(W.gridShadeCondLean), 128, 0, W.side[2]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                         k_shade<kShadeGeneric, false, false, true><<<cap(W.gridShadeLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                     } else {
                         k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, W.side[0]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                         k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, W.side[1]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
+                        k_shade<kShadeConductor><<<cap(W.gridShadeCond), 128, 0, W.side[2]>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                         k_shade<kShadeGeneric><<<cap(W.gridShade), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{});
                     }
-                    for (int k = 0; k < 2; ++k) {
+                    for (int k = 0; k < Workspace::kSide; ++k) {
                         CR_CUDA(cudaEventRecord(W.join[k], W.side[k]));
                         CR_CUDA(cudaStreamWaitEvent(s, W.join[k], 0));
                     }
-                    launches += 3;
+                    launches += 4;
                 } else {
                 if (lean) {
                     rec(1, [&] { k_shade<kShadeMiss, false, false, true><<<cap(W.gridShadeMissLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                     rec(1, [&] { k_shade<kShadeNeeNull, false, false, true><<<cap(W.gridShadeLightLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    if (dev.conductor_class)
+                        rec(1, [&] { k_shade<kShadeConductor, false, false, true><<<cap(W.gridShadeCondLean), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 } else {
                     rec(1, [&] { k_shade<kShadeMiss><<<cap(W.gridShadeMiss), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                     rec(1, [&] { k_shade<kShadeNeeNull><<<cap(W.gridShadeLight), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
+                    if (dev.conductor_class)
+                        rec(1, [&] { k_shade<kShadeConductor><<<cap(W.gridShadeCond), 128, 0, s>>>(dev, P, st, W.q, cur, C, E, W.stats, JobTable{}); });
                 }
                 if (guide) {
                     rec(1, [&] {
@@ -1038,14 +1053,16 @@ void renderNoAlloc(cr_gpu_scene& g, const cr_camera& camera, const cr_render_opt
     const bool noAlpha = !g.dev.any_alpha_mask;
     const bool lean = g.dev.texture_count == 0 && g.dev.punctual_count == 0 && !g.dev.any_alpha_mask;
     const void* traceK = noAlpha ? reinterpret_cast<const void*>(k_trace<false, false, true>) : reinterpret_cast<const void*>(k_trace<false>);
-    const void* shadeK[kShadeClasses] = {
+    // (the scene's own tables route rough conductors to the generic kernel: three classes here)
+    constexpr int kClasses = 3;
+    const void* shadeK[kClasses] = {
         lean ? reinterpret_cast<const void*>(k_shade<kShadeMiss, false, false, true>) : reinterpret_cast<const void*>(k_shade<kShadeMiss>),
         lean ? reinterpret_cast<const void*>(k_shade<kShadeNeeNull, false, false, true>) : reinterpret_cast<const void*>(k_shade<kShadeNeeNull>),
         lean ? reinterpret_cast<const void*>(k_shade<kShadeGeneric, false, false, true>) : reinterpret_cast<const void*>(k_shade<kShadeGeneric>)};
     const int gridRegen = occupancyGrid(reinterpret_cast<const void*>(k_regen<false>), 128, g.device);
     const int gridTrace = occupancyGrid(traceK, 128, g.device);
-    int gridShadeK[kShadeClasses];
-    for (int c = 0; c < kShadeClasses; ++c) gridShadeK[c] = occupancyGrid(shadeK[c], 128, g.device);
+    int gridShadeK[kClasses];
+    for (int c = 0; c < kClasses; ++c) gridShadeK[c] = occupancyGrid(shadeK[c], 128, g.device);
     const int gridSmall = sms * 8;
     // The workspace keeps the previous call's contents: clear what must start at zero.
     CR_CUDA(cudaMemsetAsync(L.acc, 0, 3 * pixels * sizeof(double), s));

@@ -354,6 +354,82 @@ CR_D BsdfSample sampleBsdf(const Surface& s, V3 wo, Rng& rng) {
     return out;
 }
 
+// ---- GGX conductor (the bsdf.cpp BSDF at metallic exactly 1, transmission exactly 0) -----------
+// A material with metallic 1, transmission 0 and no texture that could change either (the
+// kTriConductor surfaces) has, in the BSDF above: diffuse and transmission weights
+// (1 - metallic) * ... = 0 for finite factors, so the diffuse lobe's probability and the delta
+// transmission probability are 0, the micro-facet lobe's probability 1 - 0 - 0 = 1 and the
+// reflection probability r / (r + 0) = 1; the reflection colour (1 - metallic) * F + C * 1 = C.
+// The functions below are that BSDF with the exact zeros left out: the same values, pdfs and
+// random draws (the lobe and reflection draws are consumed and cannot change the outcome), so
+// the conductor shading kernel renders what the generic one renders, with far less code.
+struct CondCtx {
+    const Surface& s;
+    Frame frame;
+    V3 wo;
+    float alpha;
+    bool smooth;
+    CR_D CondCtx(const Surface& surface, V3 outgoing)
+        : s(surface), frame(dot(outgoing, surface.normal) > 0 ? surface.normal : -surface.normal) {
+        wo = frame.local(outgoing);
+        alpha = smax(0.001f, s.roughness * s.roughness);
+        smooth = s.roughness <= 0.001f;
+    }
+    CR_D V3 reflection(float cosine) const {
+        const float schlick = fpow5(1 - sclamp(fabsf(cosine), 0.0f, 1.0f));
+        return s.baseColor + (V3{1} - s.baseColor) * schlick;
+    }
+};
+CR_D BsdfEval evalConductor(const CondCtx& c, V3 wi) {
+    const BsdfEval zero{V3{}, 0};
+    const float no = c.wo.z, ni = fabsf(wi.z);
+    if (no <= 1e-7f || ni <= 1e-7f) return zero;
+    if (!(wi.z > 0) || c.smooth) return zero;  // transmission is zero; a smooth lobe is a delta
+    V3 h = normalize(c.wo + wi);
+    if (h.z < 0) h = -h;
+    const float oh = dot(c.wo, h), ih = dot(wi, h);
+    if (oh <= 0 || ih <= 0) return zero;
+    const float d = distribution(c.alpha, h), g1 = smithG1(c.alpha, c.wo), g = g1 * smithG1(c.alpha, wi);
+    const float pdfH = d * g1 * oh / no;
+    return BsdfEval{c.reflection(oh) * (d * g / (4 * no * ni)), pdfH / (4 * oh)};
+}
+CR_D BsdfEval evaluateConductor(const Surface& s, V3 wo, V3 wi) {
+    const CondCtx c(s, wo);
+    const V3 local = c.frame.local(wi);
+    if (!correctGeometricSide(s, wo, wi, local.z < 0)) return BsdfEval{V3{}, 0};
+    return evalConductor(c, local);
+}
+CR_D BsdfSample sampleConductor(const Surface& s, V3 wo, Rng& rng) {
+    const CondCtx c(s, wo);
+    BsdfSample out = emptySample();
+    if (c.wo.z <= 1e-7f) return out;
+    rng.uniform();  // the lobe draw: the micro-facet lobe has probability 1
+    const float u = rng.uniform(), v = rng.uniform();
+    const V3 h = c.smooth ? V3{0, 0, 1} : visibleNormal(c.wo, c.alpha, u, v);
+    const float oh = dot(c.wo, h);
+    rng.uniform();  // the reflection draw: reflection has probability 1
+    V3 wi = reflect(-c.wo, h);
+    if (wi.z <= 0) return out;
+    out.transmitted = false;
+    out.eta = 1;
+    if (c.smooth) {
+        out.delta = true;
+        out.direction = normalize(c.frame.world(wi));
+        if (!correctGeometricSide(s, wo, out.direction, false)) return emptySample();
+        out.pdf = 1;
+        out.weight = c.reflection(oh);
+        return out;
+    }
+    out.direction = normalize(c.frame.world(wi));
+    wi = c.frame.local(out.direction);
+    if (wi.z < 0 || !correctGeometricSide(s, wo, out.direction, false)) return emptySample();
+    const BsdfEval e = evalConductor(c, wi);
+    if (e.pdf <= 0 || !isfin(e.pdf)) return emptySample();
+    out.pdf = e.pdf;
+    out.weight = e.value * (fabsf(wi.z) / e.pdf);
+    return out;
+}
+
 // ---- environment (render.cpp:10-94) ----------------------------------------------------------
 CR_D float2 envUv(const DevScene& S, V3 d) {
     float u = (fatan2(d.z, d.x) - S.env_rotation) / (2 * kPi) + 0.5f;

@@ -12,8 +12,8 @@ sampler.
 * The film at 4096 spp against the reference's own render (committed fixture made by
   tests/golden/make_golden.py): relMSE <= 1e-4.
 * The alias table: its texel histogram against the CDF's per-texel probabilities, its
-  densities against the CDF's, its film against the CDF sampler's film, and the draws the
-  NEE-null shading class consumes for a light sample it skips.
+  densities against the CDF's and its film against the CDF sampler's film.
+* The specialised shading kernels (NEE-null and conductor classes) against the generic one.
 """
 import ctypes
 
@@ -192,10 +192,11 @@ def test_alias_film_is_unbiased_against_cdf_film(crgpu, gpu):
 
 
 @pytest.mark.parametrize("alias", [0, 1])
-def test_nee_null_class_consumes_the_light_samples_draws(crgpu, gpu, grid, alias):
+def test_specialised_shading_classes_match_the_generic_kernel(crgpu, gpu, grid, alias):
     """Hits on smooth dielectrics (the NEE-null class) skip the light sample's arithmetic but
-    must advance the stream by the same draws: the film equals the one every hit shades
-    through the generic kernel, with either environment sampler."""
+    must advance the stream by the same draws, and hits on rough conductors (the conductor
+    class) use the BSDF without its zero lobes: the film equals the one every hit shades
+    through the generic kernel, bit for bit, with either environment sampler."""
     sc, _, g = grid
     opt = crgpu.Options.make(width=160, height=90, samples=4, bounces=16, seed=42)
     a, _ = g.render(sc["camera"], opt, tuning=tuning(env_alias=alias))

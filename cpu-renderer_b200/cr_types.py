@@ -26,9 +26,9 @@ light_dtype = np.dtype([("type", "<i4"), ("position", "<f4", 3), ("direction", "
 texture_dtype = np.dtype([("image", "<i4"), ("wrap_s", "<i4"), ("wrap_t", "<i4"), ("linear", "<i4")])
 
 # cr_traced_ray: a ray a render traced and the traversal's answer (cr_gpu_render_trace_dump)
-traced_ray_dtype = np.dtype({"names": ["ray", "ignore", "kind", "depth", "found", "hit"],
-                             "formats": [ray_dtype, "<u4", "<u4", "<u4", "<u4", hit_dtype],
-                             "offsets": [0, 44, 48, 52, 56, 64], "itemsize": 96})
+traced_ray_dtype = np.dtype({"names": ["ray", "ignore", "kind", "depth", "found", "launch", "hit"],
+                             "formats": [ray_dtype, "<u4", "<u4", "<u4", "<u4", "<u4", hit_dtype],
+                             "offsets": [0, 44, 48, 52, 56, 60, 64], "itemsize": 96})
 
 assert triangle_dtype.itemsize == 188 and ray_dtype.itemsize == 44 and hit_dtype.itemsize == 32
 assert node_dtype.itemsize == 32 and material_dtype.itemsize == 220 and light_dtype.itemsize == 56

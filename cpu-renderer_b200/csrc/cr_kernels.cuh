@@ -82,8 +82,9 @@ struct JobTable {
     uint32_t refillMin;              // refill only when at least this many slots are free
 };
 
+// kStatIterations: pool iterations started (k_regen counts them; read by the ray dump).
 enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatPairs = 4, kStatTris = 5,
-       kStatIssued = 6, kStatShadowPairs = 7, kStatShadowTris = 8, kStatWords = 12 };
+       kStatIssued = 6, kStatShadowPairs = 7, kStatShadowTris = 8, kStatIterations = 9, kStatWords = 12 };
 
 CR_D uint64_t errorKey(const RenderParams& P, uint32_t pixel, uint32_t sample) {
     const uint32_t x = pixel % static_cast<uint32_t>(P.width), y = pixel / static_cast<uint32_t>(P.width);
@@ -467,7 +468,7 @@ CR_D int closestFinish(const DevScene& S, const RenderParams& P, const PathSoA& 
 
 // Records one traced ray and the traversal's answer (cr_gpu_render_trace_dump).
 CR_D void dumpRay(const TraceDump& D, const TRay& r, uint32_t ignore, uint32_t kind, uint32_t depth, bool found,
-                  const HitRec& h) {
+                  const HitRec& h, uint32_t launch) {
     const unsigned long long i = atomicAdd(D.count, 1ull);
     if (i >= D.capacity) return;
     cr_traced_ray& o = D.rays[i];
@@ -475,7 +476,7 @@ CR_D void dumpRay(const TraceDump& D, const TRay& r, uint32_t ignore, uint32_t k
     o.ray.direction[0] = r.d.x; o.ray.direction[1] = r.d.y; o.ray.direction[2] = r.d.z;
     o.ray.tmin = r.tmin; o.ray.tmax = r.tmax;
     o.ray.origin_low[0] = r.olow.x; o.ray.origin_low[1] = r.olow.y; o.ray.origin_low[2] = r.olow.z;
-    o.ignore = ignore; o.kind = kind; o.depth = depth; o.found = found ? 1u : 0u;
+    o.ignore = ignore; o.kind = kind; o.depth = depth; o.found = found ? 1u : 0u; o.launch = launch;
     o.hit.t = found ? h.t : static_cast<double>(kInf);
     o.hit.u = found ? h.u : 0.0;
     o.hit.v = found ? h.v : 0.0;
@@ -500,7 +501,8 @@ CR_D bool shadowOne(const DevScene& S, const RenderParams& P, const OutRef& O, c
     if (COUNT) {
         atomicAdd(&stats[kStatShadowPairs], static_cast<unsigned long long>(vc.pairs));
         atomicAdd(&stats[kStatShadowTris], static_cast<unsigned long long>(vc.tris));
-        if (st.dump.rays) dumpRay(st.dump, r, __float_as_uint(lo.w), 1, st.depth[path], blocked, h);
+        if (st.dump.rays) dumpRay(st.dump, r, __float_as_uint(lo.w), 1, st.depth[path], blocked, h,
+                                  static_cast<uint32_t>(stats[kStatIterations]) - 1);
     }
     return shadowFinish(P, O, st, path, E, blocked, err, c);
 }
@@ -519,7 +521,8 @@ CR_D int closestOne(const DevScene& S, const RenderParams& P, const PathSoA& st,
     if (COUNT) {
         atomicAdd(&stats[kStatPairs], static_cast<unsigned long long>(vc.pairs));
         atomicAdd(&stats[kStatTris], static_cast<unsigned long long>(vc.tris));
-        if (st.dump.rays) dumpRay(st.dump, r, st.prev_tri[path], 0, st.depth[path], found, h);
+        if (st.dump.rays) dumpRay(st.dump, r, st.prev_tri[path], 0, st.depth[path], found, h,
+                                  static_cast<uint32_t>(stats[kStatIterations]) - 1);
     }
     return closestFinish(S, P, st, path, E, found, h, err);
 }
@@ -581,6 +584,7 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         q.counts[kCountFree0 + cur] = 0;
         for (int c = 0; c < kShadeClasses; ++c) q.counts[kCountShade0 + c] = 0;
+        if (stats) stats[kStatIterations] += 1;
     }
     const uint32_t* freeQ = q.free[cur ^ 1];
     if constexpr (!MULTI) {

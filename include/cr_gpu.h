@@ -315,6 +315,7 @@ typedef struct cr_traced_ray {
     uint32_t kind;      /* 0: closest hit (any = false), 1: shadow ray (any = true)          */
     uint32_t depth;     /* the path's bounce when the ray was traced                         */
     uint32_t found;     /* the traversal's return value                                      */
+    uint32_t launch;    /* the pool iteration (traversal launch) of the render that traced it */
     cr_hit hit;         /* kind 0 and found: t, u, v, triangle as the traversal returned them */
 } cr_traced_ray;
 

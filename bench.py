@@ -51,6 +51,8 @@ def parse():
                     help="serve: iterations between the engine's host checks (0: the engine's default)")
     ap.add_argument("--mix-scale", type=float, default=1.0,
                     help="batch/serve: scale every job's width and height (quick runs)")
+    ap.add_argument("--frame", default="1920x1080",
+                    help="guided: the learned-proposal scene's frame (the 1080p workload's frame by default)")
     return ap.parse_args()
 
 
@@ -379,21 +381,29 @@ def run_batch(args):
 
     samples = sum(w * h * spp for _, _, (w, h), spp in mix)
     t0 = time.perf_counter()
-    tuning = crgpu.autotune_batch(jobs())
+    trials = []
+    tuning = crgpu.autotune_batch(jobs(), trials=trials)
     tune_s = time.perf_counter() - t0
+
+    def one_by_one_pass():
+        # each job through cr_gpu_render_resident, in the same order
+        t0 = time.perf_counter()
+        for i, (_, _, (w, h), spp) in enumerate(mix):
+            scenes[i][0].render_resident(scenes[i][1], crgpu.Options.make(width=w, height=h, samples=spp, bounces=12, seed=42))
+        return time.perf_counter() - t0
+
     for _ in range(max(0, args.warmup)):
         crgpu.render_batch(jobs(), tuning)
-    secs, est = [], None
+        one_by_one_pass()
+    # the two arms alternate, step by step, so drifts of the clock or the host hit both alike
+    secs, single, est = [], [], None
     for _ in range(args.steps):
         t0 = time.perf_counter()
         est = crgpu.render_batch(jobs(), tuning)
         secs.append(time.perf_counter() - t0)
+        single.append(one_by_one_pass())
     value = samples * len(secs) / sum(secs) / 1e6
-    # one by one: each job through cr_gpu_render_resident, in the same order
-    t0 = time.perf_counter()
-    for i, (_, _, (w, h), spp) in enumerate(mix):
-        scenes[i][0].render_resident(scenes[i][1], crgpu.Options.make(width=w, height=h, samples=spp, bounces=12, seed=42))
-    single_s = time.perf_counter() - t0
+    single_s = sum(single) / len(single)
     one_by_one = samples / single_s / 1e6
     line = {
         "metric": "aggregate Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps,
@@ -403,9 +413,11 @@ def run_batch(args):
                    "samples": int(samples), "bounces": 12, "timing": "wall clock around cr_gpu_render_batch",
                    "clutter": "literal config-1 sizes" if args.literal_clutter else "area-preserving sizes",
                    "mix_scale": args.mix_scale},
-        "one_by_one": {"value": one_by_one, "unit": "Msamples/s", "seconds": single_s},
+        "one_by_one": {"value": one_by_one, "unit": "Msamples/s", "seconds": single_s,
+                       "step_seconds": [round(x, 3) for x in single]},
+        "batch_step_seconds": [round(x, 3) for x in secs],
         "speedup_vs_one_by_one": value / one_by_one,
-        "tuning": tuning.as_dict(), "autotune_seconds": tune_s, "scene_prep_seconds": prep,
+        "tuning": tuning.as_dict(), "autotune_seconds": tune_s, "autotune_trials": trials, "scene_prep_seconds": prep,
         "engine": est,
     }
     print(json.dumps(line))
@@ -448,6 +460,7 @@ def run_serve(args):
         srv.wait(t)
     sstats = srv.stats()
     srv.close()
+    busy = sstats["seconds"]  # the engine's working time (steps), idle waits for arrivals excluded
     sub = np.array([sp.times["submitted"] for sp in specs])
     first = np.array([sp.times["first_frame"] for sp in specs])
     fin = np.array([sp.times["finished"] for sp in specs])
@@ -469,7 +482,11 @@ def run_serve(args):
                    "mix_scale": args.mix_scale, "iterations_per_step": args.engine_iters or 8},
         "time_to_first_4spp_ms": {"p50": pct(ttff, 50), "p99": pct(ttff, 99)},
         "time_to_completion_ms": {"p50": pct(ttc, 50), "p99": pct(ttc, 99)},
-        "throughput": {"served": served, "batched": batched, "unit": "Msamples/s", "served_over_batched": served / batched},
+        "throughput": {"served": served, "batched": batched, "unit": "Msamples/s", "served_over_batched": served / batched,
+                       "served_busy": samples / busy / 1e6, "served_busy_over_batched": samples / busy / 1e6 / batched,
+                       "note": "served: samples over first arrival to last completion (bounded by the arrival rate "
+                               "when the stream offers less than the device renders); served_busy: samples over the "
+                               "engine's working time"},
         "offered_load_msamples_per_s": samples / max(1e-9, stream[-1][0]) / 1e6,
         "failed": int((~ok).sum()), "server": sstats,
     }
@@ -523,8 +540,9 @@ def run_guided(args):
         return out
 
     results = {}
+    fw, fh = (int(x) for x in args.frame.split("x"))
     for name, sc, (w, h), bounces, nee, spps, ref_spp in (
-            ("caustic_sphere_grid", workloads.caustic_scene(320, 180), (320, 180), 16, True, (64, 256, 1024, 4096), 16384),
+            ("caustic_sphere_grid", workloads.caustic_scene(fw, fh), (fw, fh), 16, True, (64, 256, 1024, 4096), 16384),
             ("room_without_nee", workloads.room_scene(), (64, 64), 8, False, (256, 1024, 4096), 65536)):
         tris, _ = crgpu.finalize(sc["triangles"], sc["materials"])
         env = crgpu.env_desc(image=sc["env_image"]) if sc.get("env_image") is not None else None

@@ -161,13 +161,22 @@ class Job(C.Structure):
 class EngineTuning(C.Structure):
     _fields_ = [("pool_paths", C.c_uint32), ("range_samples", C.c_uint32), ("refill_interval", C.c_uint32),
                 ("iterations_per_step", C.c_uint32), ("use_graphs", C.c_int32), ("issue_policy", C.c_int32),
-                ("memory_budget", C.c_uint64), ("refill_free_percent", C.c_uint32), ("solo_samples_log2", C.c_uint32)]
+                ("memory_budget", C.c_uint64), ("refill_free_percent", C.c_uint32), ("solo_samples_log2", C.c_uint32),
+                ("block_size", C.c_uint32), ("reserved", C.c_uint32)]
 
     @classmethod
     def make(cls, pool_paths=0, range_samples=0, refill_interval=0, iterations_per_step=0, use_graphs=1, memory_budget=0,
-             issue_policy=0, refill_free_percent=0, solo_samples_log2=0):
+             issue_policy=0, refill_free_percent=0, solo_samples_log2=0, block_size=0):
         return cls(pool_paths, range_samples, refill_interval, iterations_per_step, use_graphs, issue_policy, memory_budget,
-                   refill_free_percent, solo_samples_log2)
+                   refill_free_percent, solo_samples_log2, block_size, 0)
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class AutotuneTrial(C.Structure):
+    _fields_ = [("pool_paths", C.c_uint32), ("iterations_per_step", C.c_uint32), ("refill_free_percent", C.c_uint32),
+                ("block_size", C.c_uint32), ("seconds", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

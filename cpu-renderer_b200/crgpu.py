@@ -11,7 +11,7 @@ import os
 import numpy as np
 
 from cr_types import (  # noqa: F401  (the layouts are part of this module's interface)
-    ALPHA_MASK, ALPHA_OPAQUE, ENCODE_HDR_FILE, ENCODE_RGBE, ENCODE_SRGB8, FRAME_FN, INF, LIGHT_DIRECTIONAL, LIGHT_POINT,
+    ALPHA_MASK, ALPHA_OPAQUE, AutotuneTrial, ENCODE_HDR_FILE, ENCODE_RGBE, ENCODE_SRGB8, FRAME_FN, INF, LIGHT_DIRECTIONAL, LIGHT_POINT,
     LIGHT_SPOT, NO_TRIANGLE, PROGRESS_FN, WRAP_CLAMP, WRAP_MIRROR, WRAP_REPEAT, Camera, EngineStats, EngineTuning,
     EnvDesc, GuideOptions, Image, Job, Options, SceneDesc, Stats, Tuning, hit_dtype, light_dtype, material_dtype,
     new_lights, new_materials, new_triangles, node_dtype, ray_dtype, slot_dtype, texture_dtype, traced_ray_dtype,
@@ -70,6 +70,8 @@ def _load():
         "cr_gpu_phase_benchmark": (C.c_int, [P, C.POINTER(Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint64, P]),
         "cr_gpu_render_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning), C.POINTER(EngineStats)]),
         "cr_gpu_autotune_batch": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning)]),
+        "cr_gpu_autotune_batch_trials": (C.c_int, [P, C.c_uint32, C.POINTER(EngineTuning), P, C.c_uint32,
+                                                   C.POINTER(C.c_uint32)]),
         "cr_server_create": (C.c_int, [C.c_int, C.POINTER(EngineTuning), C.POINTER(P)]),
         "cr_server_submit": (C.c_int, [P, P, C.POINTER(C.c_uint64)]),
         "cr_server_wait": (C.c_int, [P, C.c_uint64, C.c_double]),
@@ -421,12 +423,19 @@ def render_batch(specs, tuning=None):
     return st.as_dict()
 
 
-def autotune_batch(specs, base=None):
+def autotune_batch(specs, base=None, trials=None):
+    """cr_gpu_autotune_batch_trials: the chosen EngineTuning; the trials it ran (dicts) are
+    appended to `trials` when a list is given."""
     arr = (Job * len(specs))()
     for i, sp in enumerate(specs):
         arr[i] = sp.job
     t = base if base is not None else EngineTuning.make()
-    check(lib.cr_gpu_autotune_batch(C.cast(arr, C.c_void_p), len(specs), C.byref(t)))
+    table = (AutotuneTrial * 64)()
+    n = C.c_uint32(0)
+    check(lib.cr_gpu_autotune_batch_trials(C.cast(arr, C.c_void_p), len(specs), C.byref(t), C.cast(table, C.c_void_p),
+                                           len(table), C.byref(n)))
+    if trials is not None:
+        trials.extend(table[i].as_dict() for i in range(min(n.value, len(table))))
     return t
 
 

@@ -60,6 +60,7 @@ struct EngineConfig {
     bool graphs = true;
     int policy = 0;  // 1: jobs in order, 2: fewest samples per pixel first
     uint64_t budget = 150ull << 30;
+    int block = 128;  // threads per block of the pool's traversal and shading kernels
 };
 
 EngineConfig makeConfig(const cr_engine_tuning* t, int defaultPolicy) {
@@ -74,6 +75,7 @@ EngineConfig makeConfig(const cr_engine_tuning* t, int defaultPolicy) {
         c.graphs = t->use_graphs != 0;
         if (t->issue_policy == 1 || t->issue_policy == 2) c.policy = t->issue_policy;
         if (t->memory_budget) c.budget = t->memory_budget;
+        if (t->block_size == 64 || t->block_size == 256) c.block = static_cast<int>(t->block_size);
     }
     c.pool = std::max<uint64_t>(1024, (c.pool + 127) / 128 * 128);
     c.rangeSamples = std::max<uint64_t>(1024, c.rangeSamples);
@@ -124,6 +126,7 @@ struct Active {
     std::deque<uint32_t> ranges;  // issued, not yet summed, in sample order
     bool failed = false;
     unsigned long long errKey = kNoKey;
+    uint64_t admitStep = 0;  // the engine step that admitted the job
     std::vector<unsigned char> frame;
 };
 
@@ -145,32 +148,43 @@ class Engine {
         params_ = pool_.alloc<RenderParams>(kMaxJobSlots);
         ranges_ = pool_.alloc<IssueRange>(kMaxRanges);
         done_ = pool_.alloc<unsigned long long>(kMaxRanges);
-        ctl_ = pool_.alloc<unsigned long long>(4);  // [0] issue end, [1] range count, [2..3] issued
+        // [0] issue end, [1] range count, [2..3] issued, [4..5] free-ring head, [6] free-ring tail
+        // (host staging hCtl_: [0..1] and [2..3] alternate for the issue end and range count)
+        ctl_ = pool_.alloc<unsigned long long>(8);
         allocPaths(scratchAlloc_, 1, one_, oneQ_);
         one_.out = scratchAlloc_.alloc<float4>(1);
         oneDetail_ = scratchAlloc_.alloc<DevError>(1);
         oneStats_ = scratchAlloc_.alloc<unsigned long long>(2);
-        for (int k = 0; k < 6; ++k) crh::count_allocation();
+        for (int k = 0; k < 2 + 2 * 5; ++k) crh::count_allocation();
         CR_CUDA(cudaMallocHost(&hRanges_, kMaxRanges * sizeof(IssueRange)));
-        CR_CUDA(cudaMallocHost(&hDone_, kMaxRanges * sizeof(unsigned long long)));
-        CR_CUDA(cudaMallocHost(&hCtl_, 4 * sizeof(unsigned long long)));
-        CR_CUDA(cudaMallocHost(&hErr_, kMaxJobSlots * sizeof(unsigned long long)));
-        CR_CUDA(cudaMallocHost(&hCounts_, kCountWords * sizeof(uint32_t)));
-        CR_CUDA(cudaMallocHost(&hStats_, kStatWords * sizeof(unsigned long long)));
-        CR_CUDA(cudaMemsetAsync(ctl_, 0, 4 * sizeof(unsigned long long), s_));
+        CR_CUDA(cudaMallocHost(&hCtl_, 8 * sizeof(unsigned long long)));
+        for (Mirror& M : mirrors_) {
+            CR_CUDA(cudaMallocHost(&M.done, kMaxRanges * sizeof(unsigned long long)));
+            CR_CUDA(cudaMallocHost(&M.ctl, 4 * sizeof(unsigned long long)));
+            CR_CUDA(cudaMallocHost(&M.err, kMaxJobSlots * sizeof(unsigned long long)));
+            CR_CUDA(cudaMallocHost(&M.counts, kCountWords * sizeof(uint32_t)));
+            CR_CUDA(cudaMallocHost(&M.stats, kStatWords * sizeof(unsigned long long)));
+            CR_CUDA(cudaEventCreateWithFlags(&M.ready, cudaEventDisableTiming));
+        }
+        hDone_ = mirrors_[0].done;
+        hErr_ = mirrors_[0].err;
+        CR_CUDA(cudaMemsetAsync(ctl_, 0, 8 * sizeof(unsigned long long), s_));
         CR_CUDA(cudaMemsetAsync(done_, 0, kMaxRanges * sizeof(unsigned long long), s_));
         CR_CUDA(cudaMemsetAsync(stats_, 0, kStatWords * sizeof(unsigned long long), s_));
         CR_CUDA(cudaMemsetAsync(q_.counts, 0, kCountWords * sizeof(uint32_t), s_));
-        gridTrace_ = occupancyGrid(reinterpret_cast<const void*>(k_trace<false, true>), 128, device_);
-        gridShade_ = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric, true>), 128, device_);
-        gridLight_ = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull, true>), 128, device_);
-        gridMiss_ = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss, true>), 128, device_);
+        switch (cfg_.block) {
+            case 64: setGrids<64>(); break;
+            case 256: setGrids<256>(); break;
+            default: setGrids<128>(); break;
+        }
         gridRegen_ = occupancyGrid(reinterpret_cast<const void*>(k_regen<true>), 128, device_);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
         gridSmall_ = sms * 8;
-        k_pool_init<<<gridSmall_, 128, 0, s_>>>(q_, static_cast<uint32_t>(cfg_.pool));
+        k_pool_init<<<gridSmall_, 128, 0, s_>>>(q_, static_cast<uint32_t>(cfg_.pool));  // the ring: every slot
         CR_CUDA(cudaGetLastError());
+        hCtl_[6] = cfg_.pool;
+        CR_CUDA(cudaMemcpyAsync(ctl_ + 6, hCtl_ + 6, sizeof(unsigned long long), cudaMemcpyHostToDevice, s_));
         CR_CUDA(cudaStreamSynchronize(s_));
         for (uint32_t i = 0; i < kMaxJobSlots; ++i) freeSlots_.push_back(kMaxJobSlots - 1 - i);
         hScenes_.resize(kMaxJobSlots);
@@ -178,6 +192,10 @@ class Engine {
         J_.scenes = scenes_; J_.params = params_; J_.ranges = ranges_; J_.ctl = ctl_; J_.issued = ctl_ + 2;
         J_.done = done_; J_.errKeys = errKeys_; J_.retries = retries_; J_.range = rangeOf_;
         J_.refillMin = static_cast<uint32_t>(cfg_.pool * cfg_.refillPercent / 100);
+        J_.ring = q_.free[1];
+        J_.head = ctl_ + 4;
+        J_.tail = ctl_ + 6;
+        J_.poolSize = cfg_.pool;
     }
 
     ~Engine() {
@@ -187,8 +205,11 @@ class Engine {
         for (auto& a : active_) a.buffers.release();
         pool_.release();
         scratchAlloc_.release();
-        cudaFreeHost(hRanges_); cudaFreeHost(hDone_); cudaFreeHost(hCtl_); cudaFreeHost(hErr_);
-        cudaFreeHost(hCounts_); cudaFreeHost(hStats_);
+        cudaFreeHost(hRanges_); cudaFreeHost(hCtl_);
+        for (Mirror& M : mirrors_) {
+            cudaFreeHost(M.done); cudaFreeHost(M.ctl); cudaFreeHost(M.err); cudaFreeHost(M.counts); cudaFreeHost(M.stats);
+            if (M.ready) cudaEventDestroy(M.ready);
+        }
         if (s_) cudaStreamDestroy(s_);
     }
 
@@ -207,16 +228,29 @@ class Engine {
         return t;
     }
 
-    // One step: admit, issue, run, complete. Returns false when there is nothing to do.
+    // One step: admit, issue, run, then complete the previous step. The counters a step's
+    // graph leaves are copied to one of two host mirrors behind it, and are read after the next
+    // step's graph has been queued: the device works on step k+1 while the host completes step
+    // k (issue() sees finished ranges one step late, which only delays reuse of their space).
+    // Returns false when there is nothing to do.
     bool step() {
         CR_CUDA(cudaSetDevice(device_));
+        ++stepCount_;
         admit();
-        if (active_.empty()) return false;
+        if (active_.empty()) {
+            drainPoll();
+            return false;
+        }
         const auto t0 = std::chrono::steady_clock::now();
         issue();
         run();
-        poll();
-        complete();
+        enqueuePoll(mirror_);
+        if (pollPending_) {
+            processPoll(mirror_ ^ 1);
+            complete();
+        }
+        pollPending_ = true;
+        mirror_ ^= 1;
         std::lock_guard<std::mutex> lock(mutex_);
         busySeconds_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return true;
@@ -386,6 +420,7 @@ class Engine {
             CR_CUDA(cudaMemsetAsync(errKeys_ + a.slot, 0xff, sizeof(unsigned long long), s_));
             CR_CUDA(cudaMemsetAsync(retries_ + a.slot, 0, sizeof(unsigned long long), s_));
             usedBytes_ += a.bytes;
+            a.admitStep = stepCount_;
             j->started_at = now();
             active_.push_back(std::move(a));
             std::lock_guard<std::mutex> lock(mutex_);
@@ -399,7 +434,14 @@ class Engine {
     }
 
     void issue() {
-        // With nothing in flight the issue list starts over (positions, ranges, counters).
+        // With nothing in flight the issue list starts over (positions, ranges, counters). The
+        // counters still in flight describe the old list: they are taken first, and the test
+        // made again on them.
+        if (openRanges_ == 0 && live_ == 0 && rangeCount_ > 0 && pollPending_) {
+            processPoll(mirror_ ^ 1);
+            complete();
+            pollPending_ = false;
+        }
         if (openRanges_ == 0 && live_ == 0 && rangeCount_ > 0) {
             CR_CUDA(cudaMemsetAsync(done_, 0, rangeCount_ * sizeof(unsigned long long), s_));
             CR_CUDA(cudaMemsetAsync(ctl_ + 2, 0, 2 * sizeof(unsigned long long), s_));
@@ -428,6 +470,13 @@ class Engine {
             Active& a = *best;
             uint64_t n = std::min<uint64_t>(cfg_.rangeSamples, a.total - a.issued);
             if (a.frameSamples) n = std::min<uint64_t>(n, (a.issued / a.frameSamples + 1) * a.frameSamples - a.issued);
+            // whole samples of every pixel where a range holds at least one: issued pixel-major,
+            // so a warp's paths start samples of one pixel (as in a single render's chunks)
+            uint32_t spp = 0;
+            if (a.pixels <= n && a.issued % a.pixels == 0) {
+                n = n / a.pixels * a.pixels;
+                spp = static_cast<uint32_t>(n / a.pixels);
+            }
             uint64_t at = 0;
             if (!arena_.take(n, at)) return;
             IssueRange& R = hRanges_[rangeCount_];
@@ -437,6 +486,8 @@ class Engine {
             R.outBase = at;
             R.pixels = a.pixels;
             R.job = a.slot;
+            R.spp = spp;
+            R.s0 = spp ? static_cast<uint32_t>(a.issued / a.pixels) : 0;
             R.pad = 0;
             a.ranges.push_back(rangeCount_);
             closed_.push_back(false);
@@ -454,9 +505,12 @@ class Engine {
                                     cudaMemcpyHostToDevice, s_));
             uploaded_ = rangeCount_;
         }
-        hCtl_[0] = issueEnd_;
-        hCtl_[1] = rangeCount_;
-        CR_CUDA(cudaMemcpyAsync(ctl_, hCtl_, 2 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s_));
+        // The staging words alternate with the mirrors: the copy queued two steps ago has run
+        // (its step's counters were waited for), the one queued last step may not have.
+        unsigned long long* stage = hCtl_ + 2 * mirror_;
+        stage[0] = issueEnd_;
+        stage[1] = rangeCount_;
+        CR_CUDA(cudaMemcpyAsync(ctl_, stage, 2 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s_));
         // Kernel variant: without the alpha test when no active job's scene has alpha-masked
         // triangles, lean shading when none has textures, punctual lights or alpha masks (a job's
         // paths leave the pool before it ends, so only active jobs' paths are traced or shaded).
@@ -487,15 +541,31 @@ class Engine {
         stats_host_.launches += 5ull * cfg_.iters;
     }
 
+    template <int BLOCK>
+    void setGrids() {
+        gridTrace_ = occupancyGrid(reinterpret_cast<const void*>(k_trace<false, true, false, BLOCK>), BLOCK, device_);
+        gridShade_ = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeGeneric, true, false, false, BLOCK>), BLOCK, device_);
+        gridLight_ = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeNeeNull, true, false, false, BLOCK>), BLOCK, device_);
+        gridMiss_ = occupancyGrid(reinterpret_cast<const void*>(k_shade<kShadeMiss, true, false, false, BLOCK>), BLOCK, device_);
+    }
+
     void launchIterations(int variant) {
+        switch (cfg_.block) {
+            case 64: launchVariant<64>(variant); break;
+            case 256: launchVariant<256>(variant); break;
+            default: launchVariant<128>(variant); break;
+        }
+    }
+    template <int BLOCK>
+    void launchVariant(int variant) {
         switch (variant) {
-            case 0: launchIterationsT<false, false>(); break;
-            case 1: launchIterationsT<true, false>(); break;
-            default: launchIterationsT<true, true>(); break;  // lean implies no alpha masks
+            case 0: launchIterationsT<false, false, BLOCK>(); break;
+            case 1: launchIterationsT<true, false, BLOCK>(); break;
+            default: launchIterationsT<true, true, BLOCK>(); break;  // lean implies no alpha masks
         }
     }
 
-    template <bool NOALPHA, bool LEAN>
+    template <bool NOALPHA, bool LEAN, int BLOCK>
     void launchIterationsT() {
         const DevScene S{};
         const RenderParams P{};
@@ -505,45 +575,66 @@ class Engine {
             const int cur = static_cast<int>(i & 1);
             const int refill = (i % cfg_.refill) == 0;
             k_regen<true><<<gridRegen_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_, refill);
-            k_trace<false, true, NOALPHA><<<gridTrace_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
-            k_shade<kShadeMiss, true, false, LEAN><<<gridMiss_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
-            k_shade<kShadeNeeNull, true, false, LEAN><<<gridLight_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
-            k_shade<kShadeGeneric, true, false, LEAN><<<gridShade_, 128, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_trace<false, true, NOALPHA, BLOCK><<<gridTrace_, BLOCK, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_shade<kShadeMiss, true, false, LEAN, BLOCK><<<gridMiss_, BLOCK, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_shade<kShadeNeeNull, true, false, LEAN, BLOCK><<<gridLight_, BLOCK, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
+            k_shade<kShadeGeneric, true, false, LEAN, BLOCK><<<gridShade_, BLOCK, 0, s_>>>(S, P, st_, q_, cur, C, E, stats_, J_);
         }
         CR_CUDA(cudaGetLastError());
     }
 
-    void poll() {
-        CR_CUDA(cudaMemcpyAsync(hCounts_, q_.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s_));
-        CR_CUDA(cudaMemcpyAsync(hCtl_ + 2, ctl_ + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
+    // Copies the counters the queued graph leaves into mirror m (behind it on the stream).
+    void enqueuePoll(int m) {
+        Mirror& M = mirrors_[m];
+        CR_CUDA(cudaMemcpyAsync(M.counts, q_.counts, kCountWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, s_));
+        CR_CUDA(cudaMemcpyAsync(&M.ctl[2], ctl_ + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
+        M.first = firstOpen_;
+        M.count = rangeCount_;
+        M.step = stepCount_;
         if (rangeCount_ > firstOpen_)
-            CR_CUDA(cudaMemcpyAsync(hDone_ + firstOpen_, done_ + firstOpen_, (rangeCount_ - firstOpen_) * sizeof(unsigned long long),
+            CR_CUDA(cudaMemcpyAsync(M.done + firstOpen_, done_ + firstOpen_, (rangeCount_ - firstOpen_) * sizeof(unsigned long long),
                                     cudaMemcpyDeviceToHost, s_));
-        CR_CUDA(cudaMemcpyAsync(hErr_, errKeys_, kMaxJobSlots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
-        CR_CUDA(cudaMemcpyAsync(hStats_, stats_, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
-        CR_CUDA(cudaStreamSynchronize(s_));
+        CR_CUDA(cudaMemcpyAsync(M.err, errKeys_, kMaxJobSlots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
+        CR_CUDA(cudaMemcpyAsync(M.stats, stats_, kStatWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s_));
+        CR_CUDA(cudaEventRecord(M.ready, s_));
+    }
+    // Waits for mirror m and takes its counters as the engine's view of the pool.
+    void processPoll(int m) {
+        Mirror& M = mirrors_[m];
+        CR_CUDA(cudaEventSynchronize(M.ready));
         CR_CUDA(cudaGetLastError());
         // every step ends at parity 0: the next iteration's live queue and last shadow queue
-        live_ = static_cast<uint64_t>(hCounts_[kCountExtend0]) + hCounts_[kCountShadow1];
-        issuedPos_ = hCtl_[2];  // issued[1], written by the step's last k_regen
+        live_ = static_cast<uint64_t>(M.counts[kCountExtend0]) + M.counts[kCountShadow1];
+        issuedPos_ = M.ctl[2];  // issued[1], written by the step's last k_regen
+        hDone_ = M.done;
+        hErr_ = M.err;
+        polledRanges_ = M.count;  // ranges issued after the copy have no count in this mirror
+        polledStep_ = M.step;     // jobs admitted after it have no error key in this mirror
         std::lock_guard<std::mutex> lock(mutex_);
-        stats_host_.extend_rays = hStats_[kStatExtendRays];
-        stats_host_.shadow_rays = hStats_[kStatShadowRays];
+        stats_host_.extend_rays = M.stats[kStatExtendRays];
+        stats_host_.shadow_rays = M.stats[kStatShadowRays];
+    }
+    // Completes the step whose counters are still in flight (the pool is going idle).
+    void drainPoll() {
+        if (!pollPending_) return;
+        processPoll(mirror_ ^ 1);
+        complete();
+        pollPending_ = false;
     }
 
     void complete() {
         for (size_t k = 0; k < active_.size();) {
             Active& a = active_[k];
-            if (!a.failed && hErr_[a.slot] != kNoKey) {
+            if (!a.failed && polledStep_ >= a.admitStep && hErr_[a.slot] != kNoKey) {
                 a.failed = true;
                 a.errKey = hErr_[a.slot];
             }
             while (!a.ranges.empty()) {
                 const uint32_t r = a.ranges.front();
                 const IssueRange& R = hRanges_[r];
-                if (hDone_[r] < R.c1 - R.c0) break;
+                if (r >= polledRanges_ || hDone_[r] < R.c1 - R.c0) break;
                 if (!a.failed) {
-                    k_accumulate<<<gridSmall_, 128, 0, s_>>>(st_.out + R.outBase, Chunk{R.c0, R.c1, R.pixels}, a.acc);
+                    k_accumulate<<<gridSmall_, 128, 0, s_>>>(st_.out + R.outBase, rangeChunk(R), a.acc);
                     CR_CUDA(cudaGetLastError());
                 }
                 arena_.give(R.outBase, R.c1 - R.c0);  // reused only by launches after this one
@@ -658,10 +749,24 @@ class Engine {
     DevError* oneDetail_ = nullptr;
     unsigned long long* oneStats_ = nullptr;
     JobTable J_{};
-    // pinned host mirrors
+    // pinned host memory: the issue list, control words, and two mirrors of the counters a
+    // step leaves (hDone_ and hErr_ point into the mirror last processed)
     IssueRange* hRanges_ = nullptr;
-    unsigned long long *hDone_ = nullptr, *hCtl_ = nullptr, *hErr_ = nullptr, *hStats_ = nullptr;
-    uint32_t* hCounts_ = nullptr;
+    unsigned long long* hCtl_ = nullptr;
+    struct Mirror {
+        unsigned long long *done = nullptr, *ctl = nullptr, *err = nullptr, *stats = nullptr;
+        uint32_t* counts = nullptr;
+        uint32_t first = 0, count = 0;
+        uint64_t step = 0;
+        cudaEvent_t ready = nullptr;
+    };
+    Mirror mirrors_[2];
+    int mirror_ = 0;
+    bool pollPending_ = false;
+    uint32_t polledRanges_ = 0;
+    uint64_t stepCount_ = 0, polledStep_ = 0;
+    const unsigned long long* hDone_ = nullptr;
+    const unsigned long long* hErr_ = nullptr;
     std::vector<DevScene> hScenes_;
     std::vector<RenderParams> hParams_;
     int gridTrace_ = 0, gridShade_ = 0, gridLight_ = 0, gridMiss_ = 0, gridRegen_ = 0, gridSmall_ = 0;
@@ -771,8 +876,16 @@ cr_status cr_gpu_render_batch(cr_job* jobs, uint32_t count, const cr_engine_tuni
 }
 
 cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tuning* tuning) {
+    uint32_t n = 0;
+    return cr_gpu_autotune_batch_trials(jobs, count, tuning, nullptr, 0, &n);
+}
+
+cr_status cr_gpu_autotune_batch_trials(const cr_job* jobs, uint32_t count, cr_engine_tuning* tuning,
+                                       cr_autotune_trial* trials, uint32_t capacity, uint32_t* trialCount) {
     try {
-        if (!jobs || !tuning || count == 0) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (!jobs || !tuning || count == 0 || !trialCount || (capacity && !trials))
+            return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "NULL argument");
+        *trialCount = 0;
         // the jobs that will share the pool (larger ones render alone, see runBatch) at 1 spp
         const uint32_t soloLog2 = tuning->solo_samples_log2 ? tuning->solo_samples_log2 : kSoloSamplesLog2;
         std::vector<cr_job> trial;
@@ -791,24 +904,40 @@ cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tu
             j.every_samples = 0;
             j.on_frame = nullptr;
         }
-        const uint32_t pools[] = {1u << 22, 1u << 24};
-        const uint32_t percents[] = {0, 50, 90};
+        // one timed trial batch of the pool's jobs under t
+        auto run = [&](cr_engine_tuning t) -> double {
+            t.solo_samples_log2 = 64;  // the trial jobs are the pool's
+            const auto t0 = std::chrono::steady_clock::now();
+            const cr_status st = runBatch(trial.data(), static_cast<uint32_t>(trial.size()), &t, nullptr);
+            const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (st != CR_OK) throw crh::Error(st, std::string("autotune trial: ") + crh::last_error_text());
+            if (*trialCount < capacity)
+                trials[*trialCount] = cr_autotune_trial{t.pool_paths, t.iterations_per_step, t.refill_free_percent,
+                                                        t.block_size, sec};
+            ++*trialCount;
+            return sec;
+        };
         cr_engine_tuning best = *tuning;
-        double bestSeconds = 1e300;
-        for (uint32_t pool : pools)
-            for (uint32_t pct : percents) {
-                cr_engine_tuning t = *tuning;
-                t.pool_paths = pool;
-                t.refill_interval = 1;
-                t.refill_free_percent = pct;
-                t.iterations_per_step = 8;
-                const auto t0 = std::chrono::steady_clock::now();
-                t.solo_samples_log2 = 64;  // the trial jobs are the pool's
-                const cr_status st = runBatch(trial.data(), static_cast<uint32_t>(trial.size()), &t, nullptr);
-                const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-                if (st != CR_OK) return st;
+        if (!best.pool_paths) best.pool_paths = 1u << 24;
+        if (!best.iterations_per_step) best.iterations_per_step = 8;
+        if (!best.block_size) best.block_size = 128;
+        best.refill_interval = 1;
+        run(best);  // warm-up: scenes and device blocks touched once
+        double bestSeconds = run(best);
+        // one dimension after another, each keeping its fastest value
+        auto sweep = [&](uint32_t cr_engine_tuning::*field, std::initializer_list<uint32_t> values) {
+            for (uint32_t v : values) {
+                if (best.*field == v) continue;
+                cr_engine_tuning t = best;
+                t.*field = v;
+                const double sec = run(t);
                 if (sec < bestSeconds) { bestSeconds = sec; best = t; }
             }
+        };
+        sweep(&cr_engine_tuning::pool_paths, {1u << 22, 1u << 23, 1u << 24, 1u << 25});
+        sweep(&cr_engine_tuning::iterations_per_step, {8, 16, 32});
+        sweep(&cr_engine_tuning::refill_free_percent, {0, 50, 90});
+        sweep(&cr_engine_tuning::block_size, {64, 128, 256});
         best.solo_samples_log2 = tuning->solo_samples_log2;  // the trials ran the pool's jobs only
         *tuning = best;
         return CR_OK;

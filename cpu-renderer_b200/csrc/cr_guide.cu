@@ -1,5 +1,5 @@
-// The path-guiding network on the device: inference on the tensor cores, training (forward,
-// backward, Adam) on the CUDA cores, and the cr_guide C ABI.
+// The path-guiding network on the device: inference and training (forward and backward) on the
+// tensor cores, Adam, and the cr_guide C ABI.
 //
 // Inference (k_guide_infer): one warp evaluates 32 rows. Activations live in shared memory as
 // FP16 (row stride 72 halves), weights as FP16 [out][in] (same stride); every layer is
@@ -7,13 +7,12 @@
 // then bias + ReLU in FP32 and the result rounded back to FP16 for the next layer. The last
 // layer's 40 outputs are written as FP32.
 //
-// Training (k_guide_grad): one thread per sample computes the forward pass in FP32 with the
-// FP16-rounded weights (the values inference uses), the gradient of the weighted negative
-// log-likelihood  -w log q(dir)  with respect to the 40 outputs, and back-propagates. Weight
-// gradients of a block's 128 samples are summed in shared memory (activations and deltas of
-// all samples staged there) and added to the global gradient once per block. k_guide_adam
-// applies Adam (lr, beta1 0.9, beta2 0.999, eps 1e-8) to the FP32 masters and refreshes the
-// FP16 copy.
+// Training (k_guide_grad): a block's 64 samples go through the network as GEMMs on the tensor
+// cores (TF32 in split precision, FP32 accumulation, with the FP16-rounded weights inference
+// uses); each lane computes the gradient of its sample's weighted negative log-likelihood
+// -w log q(dir) with respect to the 40 outputs; deltas and weight gradients are GEMMs again,
+// added to the global gradient once per block. k_guide_adam applies Adam (lr, beta1 0.9,
+// beta2 0.999, eps 1e-8) to the FP32 masters and refreshes the FP16 copy.
 #include "cr_guide.cuh"
 #include "cr_driver.h"
 
@@ -218,34 +217,153 @@ __device__ float mixtureGrad(const float* out, V3 dir, float* g) {
     return -logq;
 }
 
-constexpr int kTrainThreads = 128;
+// ---- training on the tensor cores ------------------------------------------------------------
+// A block of kTrainWarps warps takes kTrainRows samples, 32 rows per warp. Every layer of the
+// forward pass, every back-propagated delta and every weight gradient is a GEMM on the tensor
+// cores: mma.sync.m16n8k8 on TF32 operands in split precision (warpGemm) with FP32
+// accumulation, operands in shared memory (FP32, row stride kTS). Forward: H = act(X W^T + b),
+// with the FP16-rounded weights inference uses. The loss gradient dL/d(outputs) of each sample
+// is computed by its own lane in FP32 (mixtureGrad). Backward: dX = (dY W) * relu'(X) per warp,
+// and dW += dY^T X, db += column sums of dY over the block's rows, added to the global gradient
+// once per block.
+constexpr int kTrainWarps = 2;
+constexpr int kTrainThreads = 32 * kTrainWarps;
+constexpr int kTrainRows = kTrainThreads;
+constexpr int kTS = 68;  // FP32 row stride: fragment loads of 8 rows x 4 columns hit 32 banks
 
-// Block-summed outer products: grad[W + n*IN + k] += sum_t D[t][n] * H[t][k], grad[B + n] += sum_t D[t][n].
-template <int NOUT, int NIN>
-__device__ void accumulateLayer(const float* D, const float* H, float* grad, int wOff, int bOff) {
-    for (int e = threadIdx.x; e < NOUT * NIN; e += blockDim.x) {
-        const int n = e / NIN, k = e % NIN;
-        float acc = 0;
-        for (int t = 0; t < kTrainThreads; ++t) acc += D[t * (kGuideWidth + 1) + n] * H[t * (kGuideWidth + 1) + k];
-        if (acc != 0.0f) atomicAdd(&grad[wOff + n * kGuideIn + k], acc);
+__device__ __forceinline__ uint32_t tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void mma1688(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                        uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+// An FP32 value as the sum of two TF32 values (hi: x rounded to TF32, lo: the rest rounded).
+struct Split { uint32_t hi, lo; };
+__device__ __forceinline__ Split split(float x) {
+    const uint32_t hi = tf32(x);
+    return Split{hi, tf32(x - __uint_as_float(hi))};
+}
+// One warp: acc[MT][NT] (16 x 8 tiles) += A (MT*16 x KT*8) times B (KT*8 x NT*8), the operands
+// read through a(m, k) and b(k, n). Each product is taken in split precision, a_hi b_hi +
+// a_hi b_lo + a_lo b_hi (three TF32 MMAs; the dropped a_lo b_lo is ~2^-22 of the product), so
+// the result has FP32 accuracy. Fragments (PTX m16n8k8, g = lane / 4, t = lane % 4):
+// A: (g, t), (g + 8, t), (g, t + 4), (g + 8, t + 4); B: (t, g), (t + 4, g);
+// C: (g, 2t), (g, 2t + 1), (g + 8, 2t), (g + 8, 2t + 1).
+template <int MT, int NT, int KT, class FA, class FB>
+__device__ __forceinline__ void warpGemm(float (&acc)[MT][NT][4], FA a, FB b) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+        const int k = kt * 8 + t;
+        Split af[MT][4];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const int m = mt * 16 + g;
+            af[mt][0] = split(a(m, k));
+            af[mt][1] = split(a(m + 8, k));
+            af[mt][2] = split(a(m, k + 4));
+            af[mt][3] = split(a(m + 8, k + 4));
+        }
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const int n = nt * 8 + g;
+            const Split b0 = split(b(k, n)), b1 = split(b(k + 4, n));
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const Split(&A)[4] = af[mt];
+                mma1688(acc[mt][nt], A[0].lo, A[1].lo, A[2].lo, A[3].lo, b0.hi, b1.hi);
+                mma1688(acc[mt][nt], A[0].hi, A[1].hi, A[2].hi, A[3].hi, b0.lo, b1.lo);
+                mma1688(acc[mt][nt], A[0].hi, A[1].hi, A[2].hi, A[3].hi, b0.hi, b1.hi);
+            }
+        }
     }
-    for (int n = threadIdx.x; n < NOUT; n += blockDim.x) {
-        float acc = 0;
-        for (int t = 0; t < kTrainThreads; ++t) acc += D[t * (kGuideWidth + 1) + n];
-        if (acc != 0.0f) atomicAdd(&grad[bOff + n], acc);
+}
+template <int MT, int NT>
+__device__ __forceinline__ void zero(float (&acc)[MT][NT][4]) {
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = acc[mt][nt][2] = acc[mt][nt][3] = 0.0f;
+}
+// Visits the accumulator's elements: f(row, col, value).
+template <int MT, int NT, class F>
+__device__ __forceinline__ void forTile(const float (&acc)[MT][NT][4], F f) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) f(mt * 16 + g + 8 * (e >> 1), nt * 8 + 2 * t + (e & 1), acc[mt][nt][e]);
+}
+
+// One warp's forward layer: Y = act(X W^T + b), X and Y 32 rows (stride kTS), W [N][64] (stride kTS).
+template <int N, bool RELU>
+__device__ void fwdLayer(const float* X, const float* W, const float* bias, float* Y) {
+    float acc[2][N / 8][4];
+    zero(acc);
+    warpGemm<2, N / 8, kGuideIn / 8>(acc, [&](int m, int k) { return X[m * kTS + k]; },
+                                     [&](int k, int n) { return W[n * kTS + k]; });
+    forTile(acc, [&](int r, int c, float v) {
+        v += bias[c];
+        Y[r * kTS + c] = RELU ? fmaxf(v, 0.0f) : v;
+    });
+    __syncwarp();
+}
+// One warp's delta through a layer: dX = (dY W) * relu'(Xact), dY 32 x NOUT, W [NOUT][64].
+template <int NOUT>
+__device__ void backLayer(const float* dY, const float* W, const float* Xact, float* dX) {
+    float acc[2][kGuideWidth / 8][4];
+    zero(acc);
+    warpGemm<2, kGuideWidth / 8, NOUT / 8>(acc, [&](int m, int k) { return dY[m * kTS + k]; },
+                                           [&](int k, int n) { return W[k * kTS + n]; });
+    forTile(acc, [&](int r, int c, float v) { dX[r * kTS + c] = Xact[r * kTS + c] > 0 ? v : 0.0f; });
+    __syncwarp();
+}
+// The block's weight and bias gradients of one layer: dW[n][k] += sum over the block's rows of
+// dY[row][n] X[row][k], db[n] += sum dY[row][n]. The warps split the output rows (16-row tiles).
+template <int NOUT>
+__device__ void weightGrad(float* const* dY, float* const* X, float* grad, int wOff, int bOff) {
+    constexpr int MT = NOUT / 16;
+    const int warp = threadIdx.x >> 5;
+    for (int mt0 = warp; mt0 < MT; mt0 += kTrainWarps) {
+        float acc[1][kGuideIn / 8][4];
+        zero(acc);
+        warpGemm<1, kGuideIn / 8, kTrainRows / 8>(
+            acc, [&](int m, int k) { return dY[k >> 5][(k & 31) * kTS + mt0 * 16 + m]; },
+            [&](int k, int n) { return X[k >> 5][(k & 31) * kTS + n]; });
+        forTile(acc, [&](int r, int c, float v) {
+            if (v != 0.0f) atomicAdd(&grad[wOff + (mt0 * 16 + r) * kGuideIn + c], v);
+        });
+    }
+    for (int n = threadIdx.x; n < NOUT; n += kTrainThreads) {
+        float a = 0;
+        for (int row = 0; row < kTrainRows; ++row) a += dY[row >> 5][(row & 31) * kTS + n];
+        if (a != 0.0f) atomicAdd(&grad[bOff + n], a);
     }
 }
 
-// samples: [n][13] = features (9), dir (3), weight. grad += d(sum_i scale * w_i * -log q_i).
+// samples: features (9), dir (3), weight. grad += d(sum_i scale * w_i * -log q_i).
 __global__ void __launch_bounds__(kTrainThreads) k_guide_grad(GuideNetDev net, const GuideSample* samples, uint64_t n,
                                                               float scale, float* grad, double* loss) {
     extern __shared__ __align__(16) unsigned char smem[];
-    float* sP = reinterpret_cast<float*>(smem);                    // kGParams
-    float* sH = sP + kGParams;                                     // [128][65] layer input
-    float* sD = sH + kTrainThreads * (kGuideWidth + 1);            // [128][65] layer delta
-    for (int i = threadIdx.x; i < kGParams; i += blockDim.x) sP[i] = net.w32[i];
-    __syncthreads();
-    const uint64_t i = blockIdx.x * static_cast<uint64_t>(kTrainThreads) + threadIdx.x;
+    float* sW = reinterpret_cast<float*>(smem);     // [kWeightRows][kTS]
+    float* sB = sW + kWeightRows * kTS;             // biases
+    float* sAct = sB + (kGParams - kGWCount);       // per warp: X, H1, H2, H3, D0, D1 (32 x kTS each)
+    for (int e = threadIdx.x; e < kWeightRows * kGuideIn; e += blockDim.x)
+        sW[(e / kGuideIn) * kTS + e % kGuideIn] = net.w32[e];
+    for (int e = threadIdx.x; e < kGParams - kGWCount; e += blockDim.x) sB[e] = net.w32[kGWCount + e];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kBuf = 32 * kTS;
+    float* my = sAct + warp * 6 * kBuf;
+    float *X = my, *H1 = my + kBuf, *H2 = my + 2 * kBuf, *H3 = my + 3 * kBuf, *D0 = my + 4 * kBuf, *D1 = my + 5 * kBuf;
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(kTrainRows) + threadIdx.x;
     const bool valid = i < n;
     float f[kGuideFeatures] = {};
     V3 dir{0, 0, 1};
@@ -256,59 +374,56 @@ __global__ void __launch_bounds__(kTrainThreads) k_guide_grad(GuideNetDev net, c
         dir = V3{smp.dir[0], smp.dir[1], smp.dir[2]};
         w = smp.weight * scale;
     }
-    float x[kGuideIn], h1[kGuideWidth], h2[kGuideWidth], h3[kGuideWidth], o[kGuideOutPad];
-    guideEncode(f, x);
-    auto dense = [&](const float* in, float* outv, int wOff, int bOff, int nout, bool relu) {
-        for (int r = 0; r < nout; ++r) {
-            float a = sP[bOff + r];
-            const float* wr = sP + wOff + r * kGuideIn;
-            for (int k = 0; k < kGuideIn; ++k) a += wr[k] * in[k];
-            outv[r] = relu ? fmaxf(a, 0.0f) : a;
-        }
-    };
-    dense(x, h1, kGW1, kGB1, kGuideWidth, true);
-    dense(h1, h2, kGW2, kGB2, kGuideWidth, true);
-    dense(h2, h3, kGW3, kGB3, kGuideWidth, true);
-    dense(h3, o, kGW4, kGB4, kGuideOutPad, false);
-    float g[kGuideOutPad];
-    for (int k = 0; k < kGuideOutPad; ++k) g[k] = 0;
-    float nll = 0;
-    if (valid && w > 0) {
-        nll = mixtureGrad(o, dir, g);
-        for (int k = 0; k < kGuideOut; ++k) g[k] *= w;
+    {
+        float x[kGuideIn];
+        guideEncode(f, x);
+        for (int k = 0; k < kGuideIn; ++k) X[lane * kTS + k] = x[k];
     }
-    if (valid) atomicAdd(loss, static_cast<double>(w * nll));
-    float* myH = sH + threadIdx.x * (kGuideWidth + 1);
-    float* myD = sD + threadIdx.x * (kGuideWidth + 1);
-    // layer 4: delta = g (48), input h3
-    for (int k = 0; k < kGuideWidth; ++k) myH[k] = h3[k];
-    for (int k = 0; k < kGuideOutPad; ++k) myD[k] = g[k];
-    __syncthreads();
-    accumulateLayer<kGuideOutPad, kGuideWidth>(sD, sH, grad, kGW4, kGB4);
-    __syncthreads();
-    float d[kGuideWidth];
-    auto backLayer = [&](const float* delta, int nout, int wOff, const float* act, float* dIn) {
-        for (int k = 0; k < kGuideWidth; ++k) {
-            float a = 0;
-            for (int r = 0; r < nout; ++r) a += sP[wOff + r * kGuideIn + k] * delta[r];
-            dIn[k] = act[k] > 0 ? a : 0.0f;  // through the ReLU of the layer that made act
+    __syncthreads();  // weights and every warp's inputs in place
+    const float* W1 = sW + (kGW1 / kGuideIn) * kTS;
+    const float* W2 = sW + (kGW2 / kGuideIn) * kTS;
+    const float* W3 = sW + (kGW3 / kGuideIn) * kTS;
+    const float* W4 = sW + (kGW4 / kGuideIn) * kTS;
+    fwdLayer<kGuideWidth, true>(X, W1, sB + (kGB1 - kGWCount), H1);
+    fwdLayer<kGuideWidth, true>(H1, W2, sB + (kGB2 - kGWCount), H2);
+    fwdLayer<kGuideWidth, true>(H2, W3, sB + (kGB3 - kGWCount), H3);
+    fwdLayer<kGuideOutPad, false>(H3, W4, sB + (kGB4 - kGWCount), D1);
+    // the loss gradient of the lane's own sample, as the delta of the output layer
+    {
+        float o[kGuideOutPad], g[kGuideOutPad];
+        for (int k = 0; k < kGuideOutPad; ++k) { o[k] = D1[lane * kTS + k]; g[k] = 0.0f; }
+        float nll = 0;
+        if (valid && w > 0) {
+            nll = mixtureGrad(o, dir, g);
+            for (int k = 0; k < kGuideOut; ++k) g[k] *= w;
         }
+        if (valid) atomicAdd(loss, static_cast<double>(w * nll));
+        for (int k = 0; k < kGuideOutPad; ++k) D0[lane * kTS + k] = g[k];
+    }
+    __syncthreads();
+    float* dYs[kTrainWarps];
+    float* Xs[kTrainWarps];
+    auto gather = [&](int buf, float** out) {
+        for (int k = 0; k < kTrainWarps; ++k) out[k] = sAct + k * 6 * kBuf + buf * kBuf;
     };
-    backLayer(g, kGuideOutPad, kGW4, h3, d);
-    for (int k = 0; k < kGuideWidth; ++k) { myH[k] = h2[k]; myD[k] = d[k]; }
+    // layer 4: dY = D0 (48 columns), input H3
+    gather(4, dYs); gather(3, Xs);
+    weightGrad<kGuideOutPad>(dYs, Xs, grad, kGW4, kGB4);
+    backLayer<kGuideOutPad>(D0, W4, H3, D1);
     __syncthreads();
-    accumulateLayer<kGuideWidth, kGuideWidth>(sD, sH, grad, kGW3, kGB3);
+    // layer 3: dY = D1, input H2
+    gather(5, dYs); gather(2, Xs);
+    weightGrad<kGuideWidth>(dYs, Xs, grad, kGW3, kGB3);
+    backLayer<kGuideWidth>(D1, W3, H2, D0);
     __syncthreads();
-    float d2[kGuideWidth];
-    backLayer(d, kGuideWidth, kGW3, h2, d2);
-    for (int k = 0; k < kGuideWidth; ++k) { myH[k] = h1[k]; myD[k] = d2[k]; }
+    // layer 2: dY = D0, input H1
+    gather(4, dYs); gather(1, Xs);
+    weightGrad<kGuideWidth>(dYs, Xs, grad, kGW2, kGB2);
+    backLayer<kGuideWidth>(D0, W2, H1, D1);
     __syncthreads();
-    accumulateLayer<kGuideWidth, kGuideWidth>(sD, sH, grad, kGW2, kGB2);
-    __syncthreads();
-    backLayer(d2, kGuideWidth, kGW2, h1, d);
-    for (int k = 0; k < kGuideWidth; ++k) { myH[k] = x[k]; myD[k] = d[k]; }
-    __syncthreads();
-    accumulateLayer<kGuideWidth, kGuideIn>(sD, sH, grad, kGW1, kGB1);
+    // layer 1: dY = D1, input X
+    gather(5, dYs); gather(0, Xs);
+    weightGrad<kGuideWidth>(dYs, Xs, grad, kGW1, kGB1);
 }
 
 __global__ void k_guide_adam(float* p, float* g, float* m, float* v, __half* p16, float* p32, int count, float lr,
@@ -337,7 +452,8 @@ __global__ void k_guide_refresh(const float* p, __half* p16, float* p32, int cou
 
 constexpr size_t kInferSmem = kWeightRows * kActStride * sizeof(__half) + (kGParams - kGWCount) * sizeof(float) +
                               kInferWarps * 32 * kActStride * sizeof(__half) + kInferWarps * 32 * kGuideOut * sizeof(float);
-constexpr size_t kTrainSmem = kGParams * sizeof(float) + 2 * kTrainThreads * (kGuideWidth + 1) * sizeof(float);
+constexpr size_t kTrainSmem = (kWeightRows * kTS + (kGParams - kGWCount) + kTrainWarps * 6 * 32 * kTS) * sizeof(float);
+static_assert(kTrainSmem <= 227 * 1024, "training block's shared memory");
 
 }  // namespace crg
 
@@ -430,7 +546,7 @@ float guideTrain(cr_guide* gd, cudaStream_t s, const GuideSample* samples, uint6
     for (uint32_t k = 0; k < steps; ++k) {
         const uint64_t count = std::min<uint64_t>(b, n - at);
         CR_CUDA(cudaMemsetAsync(gd->loss, 0, sizeof(double), s));
-        k_guide_grad<<<static_cast<unsigned>((count + kTrainThreads - 1) / kTrainThreads), kTrainThreads, kTrainSmem, s>>>(
+        k_guide_grad<<<static_cast<unsigned>((count + kTrainRows - 1) / kTrainRows), kTrainThreads, kTrainSmem, s>>>(
             gd->net(), samples + at, count, scale, gd->g, gd->loss);
         ++gd->step;
         const float bc1 = 1.0f - std::pow(0.9f, static_cast<float>(gd->step));
@@ -554,7 +670,7 @@ cr_status cr_guide_gradients(cr_guide* gd, const float* samples, uint64_t n, flo
         CR_CUDA(cudaMemcpyAsync(d, samples, n * sizeof(GuideSample), cudaMemcpyHostToDevice, gd->stream));
         CR_CUDA(cudaMemsetAsync(gd->g, 0, kGParams * sizeof(float), gd->stream));
         CR_CUDA(cudaMemsetAsync(gd->loss, 0, sizeof(double), gd->stream));
-        k_guide_grad<<<static_cast<unsigned>((n + kTrainThreads - 1) / kTrainThreads), kTrainThreads, kTrainSmem, gd->stream>>>(
+        k_guide_grad<<<static_cast<unsigned>((n + kTrainRows - 1) / kTrainRows), kTrainThreads, kTrainSmem, gd->stream>>>(
             gd->net(), d, n, 1.0f, gd->g, gd->loss);
         CR_CUDA(cudaGetLastError());
         CR_CUDA(cudaMemcpyAsync(grad, gd->g, kGParams * sizeof(float), cudaMemcpyDeviceToHost, gd->stream));

@@ -240,6 +240,7 @@ cr_status set_last_error(cr_status status, const std::string& message) {
     g_lastError = message;
     return status;
 }
+const std::string& last_error_text() { return g_lastError; }
 
 namespace {
 std::atomic<uint64_t> g_allocations{0};

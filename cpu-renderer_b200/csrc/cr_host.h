@@ -19,6 +19,7 @@ struct Error : std::runtime_error {
 };
 
 cr_status set_last_error(cr_status status, const std::string& message);
+const std::string& last_error_text();  // this thread's last message
 
 // Memory blocks the library has requested (device and page-locked host): every allocation
 // site calls count_allocation(); cr_gpu_allocation_count reports the total.

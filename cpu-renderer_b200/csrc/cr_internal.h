@@ -160,7 +160,8 @@ struct PathSoA {
     TraceDump dump;       // zero unless the render records its rays
 };
 // bits of PathSoA::flags
-enum : uint32_t { kPathLastDelta = 1u, kPathPrecise = 2u, kPathDead = 4u, kPathShadow = 8u };
+// kPathNull (alone): a multi-job pool slot whose camera sample failed; it only returns to the ring.
+enum : uint32_t { kPathLastDelta = 1u, kPathPrecise = 2u, kPathDead = 4u, kPathShadow = 8u, kPathNull = 16u };
 
 // Index queues of the path pool, each a ping-pong pair indexed by iteration parity.
 struct Queues {

@@ -64,11 +64,20 @@ CR_D void chunkSample(const Chunk& C, uint64_t j, uint32_t& pixel, uint32_t& sam
 struct IssueRange {
     uint64_t start;    // position of the range's first sample in the issue list
     uint64_t c0, c1;   // the job's sample ids [c0, c1), numbered as in a single render
-    uint64_t outBase;  // out[] index of sample id c0
+    uint64_t outBase;  // out[] index of the range's first position
     uint64_t pixels;   // the job's width * height
     uint32_t job;      // job slot
+    uint32_t spp;      // > 0: whole samples [s0, s0 + spp) of every pixel, issued pixel-major (see Chunk)
+    uint32_t s0;
     uint32_t pad;
 };
+// The range as a chunk (its positions map to pixels and samples the same way).
+CR_HD Chunk rangeChunk(const IssueRange& R) {
+    Chunk C{R.c0, R.c1, R.pixels};
+    C.spp = R.spp;
+    C.s0 = R.s0;
+    return C;
+}
 struct JobTable {
     const DevScene* scenes;          // [job slot]
     const RenderParams* params;      // [job slot]
@@ -80,7 +89,26 @@ struct JobTable {
     unsigned long long* retries;     // [job slot] precision replays
     uint32_t* range;                 // [path slot] the path's range
     uint32_t refillMin;              // refill only when at least this many slots are free
+    // The pool's free slots, a ring over `ring` (capacity `poolSize`): k_regen claims from the
+    // head (ping-pong by iteration parity, so every block of a launch reads the same head),
+    // k_trace and k_shade append the slots their paths free at the tail. k_regen never appends,
+    // so the tail it reads is the same for all its blocks.
+    uint32_t* ring;
+    unsigned long long* head;        // [2]
+    unsigned long long* tail;
+    uint64_t poolSize;
 };
+// All 32 lanes call this together: lanes with pred append slot to the pool's free ring.
+CR_D void ringPush(const JobTable& J, bool pred, uint32_t slot) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(J.tail, static_cast<unsigned long long>(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) J.ring[(base + __popc(mask & ((1u << lane) - 1u))) % J.poolSize] = slot;
+}
 
 // kStatIterations: pool iterations started (k_regen counts them; read by the ray dump).
 enum { kStatRetries = 0, kStatExtendRays = 1, kStatShadowRays = 2, kStatErrorKey = 3, kStatPairs = 4, kStatTris = 5,
@@ -542,7 +570,7 @@ CR_D PathJob pathJob(const JobTable& J, uint32_t path) {
     PathJob pj;
     pj.S = J.scenes + R.job;
     pj.P = J.params + R.job;
-    pj.O = OutRef{R.outBase - R.c0, R.pixels, 1};
+    pj.O = R.spp ? OutRef{R.outBase - R.s0, 1, R.spp} : OutRef{R.outBase - R.c0, R.pixels, 1};
     pj.E = ErrSink{J.errKeys + R.job, nullptr};
     pj.retries = J.retries + R.job;
     pj.r = r;
@@ -576,13 +604,15 @@ static __global__ void k_pool_init(Queues q, uint32_t pool) {
 
 // Free slots take the next sample ids of the chunk, in order (single render), or the next
 // positions of the issue list (MULTI: only when `refill`, and only up to the host's issue end;
-// slots left without work stay in the free queue).
+// slots left without work stay in the free ring, untouched).
 template <bool MULTI>
 __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J, int refill) {
-    const uint32_t n = q.counts[kCountFree0 + (cur ^ 1)];
+    const uint32_t n = MULTI ? 0u : q.counts[kCountFree0 + (cur ^ 1)];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        q.counts[kCountFree0 + cur] = 0;
+        // nothing appends to free[cur] in this launch (the single render's k_regen never
+        // appends, the pool's free slots are in the ring)
+        if (!MULTI) q.counts[kCountFree0 + cur] = 0;
         for (int c = 0; c < kShadeClasses; ++c) q.counts[kCountShade0 + c] = 0;
         if (stats) stats[kStatIterations] += 1;
     }
@@ -615,32 +645,36 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
         const unsigned long long end = J.ctl[0];
         const uint32_t rangeCount = static_cast<uint32_t>(J.ctl[1]);
         const uint64_t avail = end > first ? end - first : 0;
-        const uint32_t claimed = refill && n >= J.refillMin ? static_cast<uint32_t>(avail < n ? avail : n) : 0u;
-        if (blockIdx.x == 0 && threadIdx.x == 0) J.issued[cur] = first + claimed;
-        for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const unsigned long long head = J.head[cur ^ 1];
+        const uint64_t nFree = *J.tail - head;
+        const uint32_t claimed = refill && nFree >= J.refillMin ? static_cast<uint32_t>(avail < nFree ? avail : nFree) : 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            J.issued[cur] = first + claimed;
+            J.head[cur] = head + claimed;
+        }
+        for (uint32_t base = blockIdx.x * blockDim.x; base < claimed; base += gridDim.x * blockDim.x) {
             const uint32_t idx = base + threadIdx.x;
-            const bool have = idx < n;
-            const uint32_t slot = have ? freeQ[idx] : 0;
-            bool live = false, keep = false, failed = false;
+            const bool have = idx < claimed;
+            const uint32_t slot = have ? J.ring[(head + idx) % J.poolSize] : 0;
+            bool live = false, failed = false;
             uint32_t r = 0;
-            if (have && idx < claimed) {
+            if (have) {
                 const uint64_t pos = first + idx;
                 r = findRange(J, rangeCount, pos);
                 const IssueRange& R = J.ranges[r];
-                const uint64_t id = R.c0 + (pos - R.start);
-                const uint32_t pixel = static_cast<uint32_t>(id % R.pixels), sample = static_cast<uint32_t>(id / R.pixels);
+                const uint64_t j = pos - R.start;
+                uint32_t pixel, sample;
+                chunkSample(rangeChunk(R), j, pixel, sample);
                 J.range[slot] = r;
                 const ErrSink Ej{J.errKeys + R.job, nullptr};
                 live = initPath(J.scenes[R.job], J.params[R.job], st, slot, pixel, sample, false, Ej);
-                if (!live) {
-                    st.out[R.outBase + (id - R.c0)] = make_float4(0, 0, 0, 0);
-                    failed = keep = true;
+                if (!live) {  // the sample is done (radiance 0); k_trace returns the slot to the ring
+                    st.out[R.outBase + j] = make_float4(0, 0, 0, 0);
+                    st.flags[slot] = kPathNull;
+                    failed = true;
                 }
-            } else if (have) {
-                keep = true;
             }
-            warpPush(q.extend[cur], &q.counts[kCountExtend0 + cur], live, slot);
-            warpPush(q.free[cur], &q.counts[kCountFree0 + cur], keep, slot);
+            warpPush(q.extend[cur], &q.counts[kCountExtend0 + cur], have, slot);
             countDone(J, failed, r);
         }
     }
@@ -648,8 +682,10 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
 
 // Closest hit for the live queue and any hit for last iteration's shadow rays, one launch.
 // NOALPHA: no scene whose paths the launch traces has alpha-masked triangles, see accepts<NOALPHA>.
-template <bool COUNT, bool MULTI = false, bool NOALPHA = false>
-__global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+// BLOCK: threads per block (the multi-job engine tunes it; the register budget per SM, set by the
+// minimum resident blocks, stays that of 128-thread blocks).
+template <bool COUNT, bool MULTI = false, bool NOALPHA = false, int BLOCK = 128>
+__global__ void __launch_bounds__(BLOCK, CR_TRACE_MIN_BLOCKS * 128 / BLOCK) k_trace(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J) {
     const uint32_t nE = q.counts[kCountExtend0 + cur];
     const uint32_t nS = q.counts[kCountShadow0 + (cur ^ 1)];
@@ -672,8 +708,12 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
         if (idx < nE) {
             path = q.extend[cur][idx];
             if constexpr (MULTI) {
-                const PathJob pj = pathJob(J, path);
-                cls = closestOne<COUNT, NOALPHA>(*pj.S, *pj.P, st, path, pj.E, stats);
+                if (st.flags[path] == kPathNull) {
+                    freed = true;  // a sample whose camera ray failed: only its slot comes back
+                } else {
+                    const PathJob pj = pathJob(J, path);
+                    cls = closestOne<COUNT, NOALPHA>(*pj.S, *pj.P, st, path, pj.E, stats);
+                }
             } else {
                 cls = closestOne<COUNT, NOALPHA>(S, P, st, path, E, stats);
             }
@@ -687,8 +727,12 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
                 freed = shadowOne<COUNT, NOALPHA>(S, P, outOf(C), st, path, E, stats);
             }
         }
-        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
-        if constexpr (MULTI) countDone(J, freed, r);
+        if constexpr (MULTI) {
+            ringPush(J, freed, path);
+            countDone(J, freed && idx >= nE, r);  // a null path's sample was counted by k_regen
+        } else {
+            warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
+        }
 #pragma unroll
         for (int c = 0; c < kShadeClasses; ++c) warpPush(q.shade[c], &q.counts[kCountShade0 + c], cls == c, path);
     }
@@ -696,8 +740,8 @@ __global__ void __launch_bounds__(128, CR_TRACE_MIN_BLOCKS) k_trace(DevScene S, 
 
 // LEAN (every scene whose paths the launch shades has no textures, punctual lights or alpha
 // masks): the shading code without those features, a smaller kernel with the same arithmetic.
-template <int CLASS, bool MULTI = false, bool GUIDED = false, bool LEAN = false>
-__global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
+template <int CLASS, bool MULTI = false, bool GUIDED = false, bool LEAN = false, int BLOCK = 128>
+__global__ void __launch_bounds__(BLOCK, CR_SHADE_MIN_BLOCKS * 128 / BLOCK) k_shade(DevScene S, RenderParams P, PathSoA st, Queues q, int cur, Chunk C, ErrSink E,
                                                unsigned long long* stats, JobTable J) {
     const uint32_t n = q.counts[kCountShade0 + CLASS];
     const uint32_t* in = q.shade[CLASS];
@@ -718,8 +762,12 @@ __global__ void __launch_bounds__(128, CR_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
         }
         warpPush(q.extend[cur ^ 1], &q.counts[kCountExtend0 + (cur ^ 1)], cont, path);
         warpPush(q.shadow[cur], &q.counts[kCountShadow0 + cur], shadow, path);
-        warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
-        if constexpr (MULTI) countDone(J, freed, r);
+        if constexpr (MULTI) {
+            ringPush(J, freed, path);
+            countDone(J, freed, r);
+        } else {
+            warpPush(q.free[cur], &q.counts[kCountFree0 + cur], freed, path);
+        }
     }
 }
 

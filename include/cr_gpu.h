@@ -518,6 +518,9 @@ typedef struct cr_engine_tuning {
                                      fills the pool on its own and renders alone (the single-
                                      render path), before the pool takes the rest; 0: n = 24;
                                      64 or more: every job shares the pool. Servers ignore it  */
+    uint32_t block_size;          /* threads per block of the pool's traversal and shading
+                                     kernels: 64, 128 or 256; 0: 128                          */
+    uint32_t reserved;            /* must be 0                                                */
 } cr_engine_tuning;
 
 typedef struct cr_engine_stats {
@@ -532,9 +535,24 @@ typedef struct cr_engine_stats {
 cr_status cr_gpu_render_batch(cr_job* jobs, uint32_t count, const cr_engine_tuning* tuning,
                               cr_engine_stats* stats);
 
-/* Picks pool size and refill threshold for a batch by timing short trial renders (the jobs
- * at 1 sample per pixel) of candidate settings. The jobs are not modified. */
+/* The engine's own autotuner (no counterpart in the reference): picks the pool's queue depth
+ * (pool_paths), its regroup interval (iterations_per_step: iterations between the host's
+ * regrouping of finished ranges and new issue ranges), its refill threshold and the kernels'
+ * block size by timing short trial renders (the jobs that share the pool, at 1 sample per
+ * pixel), one dimension after another starting from *tuning, each keeping the fastest value.
+ * The jobs are not modified. */
 cr_status cr_gpu_autotune_batch(const cr_job* jobs, uint32_t count, cr_engine_tuning* tuning);
+
+/* One trial of the autotuner: the settings and the wall time of its trial batch. */
+typedef struct cr_autotune_trial {
+    uint32_t pool_paths, iterations_per_step, refill_free_percent, block_size;
+    double seconds;
+} cr_autotune_trial;
+/* As cr_gpu_autotune_batch, and the trials it ran: the first `capacity` go to trials,
+ * *trial_count receives how many ran. */
+cr_status cr_gpu_autotune_batch_trials(const cr_job* jobs, uint32_t count, cr_engine_tuning* tuning,
+                                       cr_autotune_trial* trials, uint32_t capacity,
+                                       uint32_t* trial_count);
 
 /* Continuous batching: a server owns an engine thread on `device`. Jobs submitted while
  * others run join the pool as soon as the memory budget admits them; their samples share the

@@ -51,6 +51,9 @@ def parse():
                     help="serve: iterations between the engine's host checks (0: the engine's default)")
     ap.add_argument("--mix-scale", type=float, default=1.0,
                     help="batch/serve: scale every job's width and height (quick runs)")
+    ap.add_argument("--solo-log2", type=int, default=0,
+                    help="batch: jobs of at least 2^n samples render alone beside the pool (0: the library's 24; "
+                         "64: every job shares the pool)")
     ap.add_argument("--frame", default="1920x1080",
                     help="guided: the learned-proposal scene's frame (the 1080p workload's frame by default)")
     return ap.parse_args()
@@ -382,7 +385,7 @@ def run_batch(args):
     samples = sum(w * h * spp for _, _, (w, h), spp in mix)
     t0 = time.perf_counter()
     trials = []
-    tuning = crgpu.autotune_batch(jobs(), trials=trials)
+    tuning = crgpu.autotune_batch(jobs(), base=crgpu.EngineTuning.make(solo_samples_log2=args.solo_log2), trials=trials)
     tune_s = time.perf_counter() - t0
 
     def one_by_one_pass():

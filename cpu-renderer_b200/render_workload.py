@@ -1,5 +1,8 @@
 """Render one of the synthetic workloads on the GPU and print the render statistics as JSON.
 
+The command line the ncu summaries under profiles/ are taken with (one render, no timing
+loop around it); bench.py is the measurement.
+
     python cpu-renderer_b200/render_workload.py --workload grid [--width 1920 --height 1080]
         [--spp 64] [--bounces 16] [--repeat 1] [--exact] [--time-phases] [--count] [--out film.npy]
 

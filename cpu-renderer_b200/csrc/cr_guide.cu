@@ -7,9 +7,8 @@
 // then bias + ReLU in FP32 and the result rounded back to FP16 for the next layer. The last
 // layer's 40 outputs are written as FP32.
 //
-// Training (k_guide_grad): a block's 64 samples go through the network as GEMMs on the tensor
-// cores (TF32 in split precision, FP32 accumulation, with the FP16-rounded weights inference
-// uses); each lane computes the gradient of its sample's weighted negative log-likelihood
+// Training (k_guide_grad): a block's 128 samples go through the network as GEMMs on the tensor
+// cores (TF32 in split precision, FP32 accumulation, with the FP16 weights inference uses); each lane computes the gradient of its sample's weighted negative log-likelihood
 // -w log q(dir) with respect to the 40 outputs; deltas and weight gradients are GEMMs again,
 // added to the global gradient once per block. k_guide_adam applies Adam (lr, beta1 0.9,
 // beta2 0.999, eps 1e-8) to the FP32 masters and refreshes the FP16 copy.
@@ -226,7 +225,7 @@ __device__ float mixtureGrad(const float* out, V3 dir, float* g) {
 // is computed by its own lane in FP32 (mixtureGrad). Backward: dX = (dY W) * relu'(X) per warp,
 // and dW += dY^T X, db += column sums of dY over the block's rows, added to the global gradient
 // once per block.
-constexpr int kTrainWarps = 2;
+constexpr int kTrainWarps = 4;
 constexpr int kTrainThreads = 32 * kTrainWarps;
 constexpr int kTrainRows = kTrainThreads;
 constexpr int kTS = 68;  // FP32 row stride: fragment loads of 8 rows x 4 columns hit 32 banks
@@ -255,7 +254,9 @@ __device__ __forceinline__ Split split(float x) {
 // the result has FP32 accuracy. Fragments (PTX m16n8k8, g = lane / 4, t = lane % 4):
 // A: (g, t), (g + 8, t), (g, t + 4), (g + 8, t + 4); B: (t, g), (t + 4, g);
 // C: (g, 2t), (g, 2t + 1), (g + 8, 2t), (g + 8, 2t + 1).
-template <int MT, int NT, int KT, class FA, class FB>
+// BEXACT: every B value is exactly a TF32 value (an FP16 weight), so its lo part is zero and
+// the a_hi b_lo product is left out.
+template <int MT, int NT, int KT, bool BEXACT = false, class FA, class FB>
 __device__ __forceinline__ void warpGemm(float (&acc)[MT][NT][4], FA a, FB b) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
 #pragma unroll
@@ -278,7 +279,7 @@ __device__ __forceinline__ void warpGemm(float (&acc)[MT][NT][4], FA a, FB b) {
             for (int mt = 0; mt < MT; ++mt) {
                 const Split(&A)[4] = af[mt];
                 mma1688(acc[mt][nt], A[0].lo, A[1].lo, A[2].lo, A[3].lo, b0.hi, b1.hi);
-                mma1688(acc[mt][nt], A[0].hi, A[1].hi, A[2].hi, A[3].hi, b0.lo, b1.lo);
+                if (!BEXACT) mma1688(acc[mt][nt], A[0].hi, A[1].hi, A[2].hi, A[3].hi, b0.lo, b1.lo);
                 mma1688(acc[mt][nt], A[0].hi, A[1].hi, A[2].hi, A[3].hi, b0.hi, b1.hi);
             }
         }
@@ -303,13 +304,14 @@ __device__ __forceinline__ void forTile(const float (&acc)[MT][NT][4], F f) {
             for (int e = 0; e < 4; ++e) f(mt * 16 + g + 8 * (e >> 1), nt * 8 + 2 * t + (e & 1), acc[mt][nt][e]);
 }
 
-// One warp's forward layer: Y = act(X W^T + b), X and Y 32 rows (stride kTS), W [N][64] (stride kTS).
+// One warp's forward layer: Y = act(X W^T + b), X and Y 32 rows (stride kTS), W [N][64] FP16
+// (stride kActStride).
 template <int N, bool RELU>
-__device__ void fwdLayer(const float* X, const float* W, const float* bias, float* Y) {
+__device__ void fwdLayer(const float* X, const __half* W, const float* bias, float* Y) {
     float acc[2][N / 8][4];
     zero(acc);
-    warpGemm<2, N / 8, kGuideIn / 8>(acc, [&](int m, int k) { return X[m * kTS + k]; },
-                                     [&](int k, int n) { return W[n * kTS + k]; });
+    warpGemm<2, N / 8, kGuideIn / 8, true>(acc, [&](int m, int k) { return X[m * kTS + k]; },
+                                           [&](int k, int n) { return __half2float(W[n * kActStride + k]); });
     forTile(acc, [&](int r, int c, float v) {
         v += bias[c];
         Y[r * kTS + c] = RELU ? fmaxf(v, 0.0f) : v;
@@ -318,51 +320,60 @@ __device__ void fwdLayer(const float* X, const float* W, const float* bias, floa
 }
 // One warp's delta through a layer: dX = (dY W) * relu'(Xact), dY 32 x NOUT, W [NOUT][64].
 template <int NOUT>
-__device__ void backLayer(const float* dY, const float* W, const float* Xact, float* dX) {
+__device__ void backLayer(const float* dY, const __half* W, const float* Xact, float* dX) {
     float acc[2][kGuideWidth / 8][4];
     zero(acc);
-    warpGemm<2, kGuideWidth / 8, NOUT / 8>(acc, [&](int m, int k) { return dY[m * kTS + k]; },
-                                           [&](int k, int n) { return W[k * kTS + n]; });
+    warpGemm<2, kGuideWidth / 8, NOUT / 8, true>(acc, [&](int m, int k) { return dY[m * kTS + k]; },
+                                                 [&](int k, int n) { return __half2float(W[k * kActStride + n]); });
     forTile(acc, [&](int r, int c, float v) { dX[r * kTS + c] = Xact[r * kTS + c] > 0 ? v : 0.0f; });
     __syncwarp();
 }
 // The block's weight and bias gradients of one layer: dW[n][k] += sum over the block's rows of
 // dY[row][n] X[row][k], db[n] += sum dY[row][n]. The warps split the output rows (16-row tiles).
+// Buffer b of warp w's activation space, and its row r.
+constexpr int kTrainBufs = 5;
+constexpr int kBuf = 32 * kTS;
+__device__ __forceinline__ float* rowOf(float* acts, int w, int b, int r) {
+    return acts + (w * kTrainBufs + b) * kBuf + r * kTS;
+}
 template <int NOUT>
-__device__ void weightGrad(float* const* dY, float* const* X, float* grad, int wOff, int bOff) {
+__device__ void weightGrad(float* acts, int dYbuf, int Xbuf, float* grad, int wOff, int bOff) {
     constexpr int MT = NOUT / 16;
     const int warp = threadIdx.x >> 5;
     for (int mt0 = warp; mt0 < MT; mt0 += kTrainWarps) {
         float acc[1][kGuideIn / 8][4];
         zero(acc);
         warpGemm<1, kGuideIn / 8, kTrainRows / 8>(
-            acc, [&](int m, int k) { return dY[k >> 5][(k & 31) * kTS + mt0 * 16 + m]; },
-            [&](int k, int n) { return X[k >> 5][(k & 31) * kTS + n]; });
+            acc, [&](int m, int k) { return rowOf(acts, k >> 5, dYbuf, k & 31)[mt0 * 16 + m]; },
+            [&](int k, int n) { return rowOf(acts, k >> 5, Xbuf, k & 31)[n]; });
         forTile(acc, [&](int r, int c, float v) {
             if (v != 0.0f) atomicAdd(&grad[wOff + (mt0 * 16 + r) * kGuideIn + c], v);
         });
     }
     for (int n = threadIdx.x; n < NOUT; n += kTrainThreads) {
         float a = 0;
-        for (int row = 0; row < kTrainRows; ++row) a += dY[row >> 5][(row & 31) * kTS + n];
+        for (int row = 0; row < kTrainRows; ++row) a += rowOf(acts, row >> 5, dYbuf, row & 31)[n];
         if (a != 0.0f) atomicAdd(&grad[bOff + n], a);
     }
 }
 
 // samples: features (9), dir (3), weight. grad += d(sum_i scale * w_i * -log q_i).
+// Per warp five activation buffers A..E (32 rows each): forward X -> A, H1 -> B, H2 -> C,
+// H3 -> D, outputs -> E; the loss gradient -> A; deltas: layer 4 -> E, layer 3 -> A, layer 2
+// -> E; the inputs X are encoded again into A for the first layer's weight gradient.
 __global__ void __launch_bounds__(kTrainThreads) k_guide_grad(GuideNetDev net, const GuideSample* samples, uint64_t n,
                                                               float scale, float* grad, double* loss) {
     extern __shared__ __align__(16) unsigned char smem[];
-    float* sW = reinterpret_cast<float*>(smem);     // [kWeightRows][kTS]
-    float* sB = sW + kWeightRows * kTS;             // biases
-    float* sAct = sB + (kGParams - kGWCount);       // per warp: X, H1, H2, H3, D0, D1 (32 x kTS each)
+    __half* sW = reinterpret_cast<__half*>(smem);                              // [kWeightRows][kActStride]
+    float* sB = reinterpret_cast<float*>(sW + kWeightRows * kActStride);      // biases
+    float* acts = sB + (kGParams - kGWCount);                                 // kTrainWarps x kTrainBufs x 32 rows
     for (int e = threadIdx.x; e < kWeightRows * kGuideIn; e += blockDim.x)
-        sW[(e / kGuideIn) * kTS + e % kGuideIn] = net.w32[e];
+        sW[(e / kGuideIn) * kActStride + e % kGuideIn] = net.w16[e];
     for (int e = threadIdx.x; e < kGParams - kGWCount; e += blockDim.x) sB[e] = net.w32[kGWCount + e];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int kBuf = 32 * kTS;
-    float* my = sAct + warp * 6 * kBuf;
-    float *X = my, *H1 = my + kBuf, *H2 = my + 2 * kBuf, *H3 = my + 3 * kBuf, *D0 = my + 4 * kBuf, *D1 = my + 5 * kBuf;
+    enum { A = 0, B = 1, C = 2, D = 3, E = 4 };
+    float* buf[kTrainBufs];
+    for (int b = 0; b < kTrainBufs; ++b) buf[b] = rowOf(acts, warp, b, 0);
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(kTrainRows) + threadIdx.x;
     const bool valid = i < n;
     float f[kGuideFeatures] = {};
@@ -374,56 +385,50 @@ __global__ void __launch_bounds__(kTrainThreads) k_guide_grad(GuideNetDev net, c
         dir = V3{smp.dir[0], smp.dir[1], smp.dir[2]};
         w = smp.weight * scale;
     }
-    {
+    auto encodeInto = [&](float* X) {
         float x[kGuideIn];
         guideEncode(f, x);
         for (int k = 0; k < kGuideIn; ++k) X[lane * kTS + k] = x[k];
-    }
+    };
+    encodeInto(buf[A]);
     __syncthreads();  // weights and every warp's inputs in place
-    const float* W1 = sW + (kGW1 / kGuideIn) * kTS;
-    const float* W2 = sW + (kGW2 / kGuideIn) * kTS;
-    const float* W3 = sW + (kGW3 / kGuideIn) * kTS;
-    const float* W4 = sW + (kGW4 / kGuideIn) * kTS;
-    fwdLayer<kGuideWidth, true>(X, W1, sB + (kGB1 - kGWCount), H1);
-    fwdLayer<kGuideWidth, true>(H1, W2, sB + (kGB2 - kGWCount), H2);
-    fwdLayer<kGuideWidth, true>(H2, W3, sB + (kGB3 - kGWCount), H3);
-    fwdLayer<kGuideOutPad, false>(H3, W4, sB + (kGB4 - kGWCount), D1);
+    const __half* W1 = sW + (kGW1 / kGuideIn) * kActStride;
+    const __half* W2 = sW + (kGW2 / kGuideIn) * kActStride;
+    const __half* W3 = sW + (kGW3 / kGuideIn) * kActStride;
+    const __half* W4 = sW + (kGW4 / kGuideIn) * kActStride;
+    fwdLayer<kGuideWidth, true>(buf[A], W1, sB + (kGB1 - kGWCount), buf[B]);
+    fwdLayer<kGuideWidth, true>(buf[B], W2, sB + (kGB2 - kGWCount), buf[C]);
+    fwdLayer<kGuideWidth, true>(buf[C], W3, sB + (kGB3 - kGWCount), buf[D]);
+    fwdLayer<kGuideOutPad, false>(buf[D], W4, sB + (kGB4 - kGWCount), buf[E]);
     // the loss gradient of the lane's own sample, as the delta of the output layer
     {
         float o[kGuideOutPad], g[kGuideOutPad];
-        for (int k = 0; k < kGuideOutPad; ++k) { o[k] = D1[lane * kTS + k]; g[k] = 0.0f; }
+        for (int k = 0; k < kGuideOutPad; ++k) { o[k] = buf[E][lane * kTS + k]; g[k] = 0.0f; }
         float nll = 0;
         if (valid && w > 0) {
             nll = mixtureGrad(o, dir, g);
             for (int k = 0; k < kGuideOut; ++k) g[k] *= w;
         }
         if (valid) atomicAdd(loss, static_cast<double>(w * nll));
-        for (int k = 0; k < kGuideOutPad; ++k) D0[lane * kTS + k] = g[k];
+        for (int k = 0; k < kGuideOutPad; ++k) buf[A][lane * kTS + k] = g[k];
     }
     __syncthreads();
-    float* dYs[kTrainWarps];
-    float* Xs[kTrainWarps];
-    auto gather = [&](int buf, float** out) {
-        for (int k = 0; k < kTrainWarps; ++k) out[k] = sAct + k * 6 * kBuf + buf * kBuf;
-    };
-    // layer 4: dY = D0 (48 columns), input H3
-    gather(4, dYs); gather(3, Xs);
-    weightGrad<kGuideOutPad>(dYs, Xs, grad, kGW4, kGB4);
-    backLayer<kGuideOutPad>(D0, W4, H3, D1);
+    // layer 4: delta A (48 columns), input H3 = D
+    weightGrad<kGuideOutPad>(acts, A, D, grad, kGW4, kGB4);
+    backLayer<kGuideOutPad>(buf[A], W4, buf[D], buf[E]);
     __syncthreads();
-    // layer 3: dY = D1, input H2
-    gather(5, dYs); gather(2, Xs);
-    weightGrad<kGuideWidth>(dYs, Xs, grad, kGW3, kGB3);
-    backLayer<kGuideWidth>(D1, W3, H2, D0);
+    // layer 3: delta E, input H2 = C
+    weightGrad<kGuideWidth>(acts, E, C, grad, kGW3, kGB3);
+    backLayer<kGuideWidth>(buf[E], W3, buf[C], buf[A]);
     __syncthreads();
-    // layer 2: dY = D0, input H1
-    gather(4, dYs); gather(1, Xs);
-    weightGrad<kGuideWidth>(dYs, Xs, grad, kGW2, kGB2);
-    backLayer<kGuideWidth>(D0, W2, H1, D1);
+    // layer 2: delta A, input H1 = B
+    weightGrad<kGuideWidth>(acts, A, B, grad, kGW2, kGB2);
+    backLayer<kGuideWidth>(buf[A], W2, buf[B], buf[E]);
+    __syncthreads();  // every warp is done with A
+    encodeInto(buf[A]);
     __syncthreads();
-    // layer 1: dY = D1, input X
-    gather(5, dYs); gather(0, Xs);
-    weightGrad<kGuideWidth>(dYs, Xs, grad, kGW1, kGB1);
+    // layer 1: delta E, input X = A
+    weightGrad<kGuideWidth>(acts, E, A, grad, kGW1, kGB1);
 }
 
 __global__ void k_guide_adam(float* p, float* g, float* m, float* v, __half* p16, float* p32, int count, float lr,
@@ -452,7 +457,8 @@ __global__ void k_guide_refresh(const float* p, __half* p16, float* p32, int cou
 
 constexpr size_t kInferSmem = kWeightRows * kActStride * sizeof(__half) + (kGParams - kGWCount) * sizeof(float) +
                               kInferWarps * 32 * kActStride * sizeof(__half) + kInferWarps * 32 * kGuideOut * sizeof(float);
-constexpr size_t kTrainSmem = (kWeightRows * kTS + (kGParams - kGWCount) + kTrainWarps * 6 * 32 * kTS) * sizeof(float);
+constexpr size_t kTrainSmem = kWeightRows * kActStride * sizeof(__half) +
+                              ((kGParams - kGWCount) + kTrainWarps * kTrainBufs * 32 * kTS) * sizeof(float);
 static_assert(kTrainSmem <= 227 * 1024, "training block's shared memory");
 
 }  // namespace crg

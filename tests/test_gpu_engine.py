@@ -233,9 +233,19 @@ def test_server_wait_timeout_and_budget(crgpu, world):
 
 
 def test_autotune_picks_a_measured_setting(crgpu, world):
+    """The autotuner searches queue depth, regroup interval, refill threshold and block size
+    one after another and returns the fastest trial it ran."""
     jobs = _mixed_jobs(crgpu, world)
-    t = autotune_batch(jobs)
-    assert t.pool_paths in (1 << 22, 1 << 24) and t.refill_free_percent in (0, 50, 90)
+    trials = []
+    t = autotune_batch(jobs, trials=trials)
+    assert t.pool_paths in (1 << 22, 1 << 23, 1 << 24, 1 << 25) and t.refill_free_percent in (0, 50, 90)
+    assert t.iterations_per_step in (8, 16, 32) and t.block_size in (64, 128, 256)
+    assert len(trials) >= 11
+    assert {tr["block_size"] for tr in trials} == {64, 128, 256}
+    timed = trials[1:]  # the first trial warms the scenes and device blocks
+    best = min(timed, key=lambda tr: tr["seconds"])
+    assert (t.pool_paths, t.iterations_per_step, t.refill_free_percent, t.block_size) == (
+        best["pool_paths"], best["iterations_per_step"], best["refill_free_percent"], best["block_size"])
     stats = render_batch(jobs, t)
     assert stats["jobs_done"] == len(jobs)
     for j in jobs:

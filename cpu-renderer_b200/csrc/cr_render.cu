@@ -615,10 +615,11 @@ void renderImpl(cr_gpu_scene& g, const cr_camera& camera, const cr_render_option
     // 1M-triangle 1080p workload that measured faster than refilling (regeneration) at every
     // pool/chunk ratio tried (212 vs 200 Msamples/s at its best, 2x pool), and a larger pool
     // amortises the drain tail over more samples (132.7 M samples at 1080p x 64 spp: 2^24 slots
-    // 526 ms, 2^25 508 ms, 2^26 499 ms, 2^27 494 ms; 2^26 slots hold ~20 GB of path state, 2^27
-    // twice that for 1 %).
+    // 526 ms, 2^25 508 ms, 2^26 499 ms, 2^27 494 ms). With pixel-major chunks 2^27 slots take
+    // all 64 samples of a 1080p frame in one chunk, one drain instead of two: 316.7 -> 320.8
+    // Msamples/s, for ~33 GB of path state (248 bytes per slot) on a 180 GB device.
     uint64_t pool = tuning.paths_per_wave > 0 ? static_cast<uint64_t>(tuning.paths_per_wave)
-                                              : (uint64_t{1} << (guide ? 23 : 26));
+                                              : (uint64_t{1} << (guide ? 23 : 27));
     pool = std::max<uint64_t>(1024, std::min<uint64_t>(pool, total));
     const uint64_t chunkBudget = uint64_t{1} << 28;  // 268 M samples = 4 GiB of float4 radiance
     if (tuning.chunk_log2 && (tuning.chunk_log2 < 16 || tuning.chunk_log2 > 28))

@@ -516,7 +516,7 @@ typedef struct cr_engine_tuning {
                                      (new paths then start together, as one wave); 0: always   */
     uint32_t solo_samples_log2;   /* cr_gpu_render_batch: a job of at least 2^n camera samples
                                      fills the pool on its own and renders alone (the single-
-                                     render path), before the pool takes the rest; 0: n = 24;
+                                     render path), before the pool takes the rest; 0: n = 22;
                                      64 or more: every job shares the pool. Servers ignore it  */
     uint32_t block_size;          /* threads per block of the pool's traversal and shading
                                      kernels: 64, 128 or 256; 0: 128                          */

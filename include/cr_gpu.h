@@ -514,10 +514,13 @@ typedef struct cr_engine_tuning {
     uint64_t memory_budget;       /* bytes of job buffers admitted at once; 0: 150 GB          */
     uint32_t refill_free_percent; /* refill only when at least this share of the pool is free
                                      (new paths then start together, as one wave); 0: always   */
-    uint32_t solo_samples_log2;   /* cr_gpu_render_batch: a job of at least 2^n camera samples
-                                     fills the pool on its own and renders alone (the single-
-                                     render path), before the pool takes the rest; 0: n = 22;
-                                     64 or more: every job shares the pool. Servers ignore it  */
+    uint32_t solo_samples_log2;   /* cr_gpu_render_batch: a job with at least 2^n camera
+                                     samples between two drains (the whole job; for a
+                                     progressive job, every_samples x pixels) fills the device
+                                     on its own and renders alone (the single-render path) on a
+                                     helper thread beside the pool, which takes the rest;
+                                     0: n = 22; 64 or more: every job shares the pool. Servers
+                                     ignore it                                                 */
     uint32_t block_size;          /* threads per block of the pool's traversal and shading
                                      kernels: 64, 128 or 256; 0: 128                          */
     uint32_t reserved;            /* must be 0                                                */

@@ -81,8 +81,9 @@ def test_batch_films_equal_single_renders(crgpu, world, tuning):
 
 
 def test_batch_solo_jobs(crgpu, world):
-    """Jobs of at least 2^solo_samples_log2 samples render alone through the single-render path
-    (here 2^14: the 64x48x16, 160x90x4 and 128x128x2 jobs), the rest share the pool; every film,
+    """Jobs of at least 2^solo_samples_log2 samples between two drains render alone through the
+    single-render path (here 2^14: the 64x48x16, 160x90x4 and 128x128x2 jobs, and the
+    progressive 64x64 job, whose 4-spp frame interval is 2^14 samples), the rest share the pool; every film,
     status and sample count is the standalone render's, and progressive frames and failures
     of solo jobs are reported as for pooled ones."""
     jobs = _mixed_jobs(crgpu, world)

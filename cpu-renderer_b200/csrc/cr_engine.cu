@@ -6,8 +6,9 @@
 //
 //   admit     a job gets a slot in the device job tables (its scene's DevScene and its
 //             RenderParams), FP64 pixel sums and a film, if the memory budget allows
-//   issue     the jobs' remaining samples are cut into ranges (at most range_samples, never
-//             across a progressive frame boundary) and appended to the issue list, each to
+//   issue     the jobs' remaining samples are cut into ranges (at most range_samples: blocks
+//             of pixels with all their samples, or for a progressive job whole samples of
+//             every pixel, never across a frame boundary) and appended to the issue list, each to
 //             the job with the fewest samples per pixel issued, while the per-sample
 //             radiance arena has room and the pool is not already fed a pool's worth ahead
 //   run       iterations_per_step iterations of k_regen / k_trace / k_shade x3 (one CUDA
@@ -140,7 +141,7 @@ class Engine {
         arena_ = Arena(cfg_.outSamples);
         allocPaths(pool_, cfg_.pool, st_, q_);
         st_.out = pool_.alloc<float4>(cfg_.outSamples);
-        rangeOf_ = pool_.alloc<uint32_t>(cfg_.pool);
+        slotOf_ = pool_.alloc<uint2>(cfg_.pool);
         stats_ = pool_.alloc<unsigned long long>(kStatWords);
         errKeys_ = pool_.alloc<unsigned long long>(kMaxJobSlots);
         retries_ = pool_.alloc<unsigned long long>(kMaxJobSlots);
@@ -190,7 +191,7 @@ class Engine {
         hScenes_.resize(kMaxJobSlots);
         hParams_.resize(kMaxJobSlots);
         J_.scenes = scenes_; J_.params = params_; J_.ranges = ranges_; J_.ctl = ctl_; J_.issued = ctl_ + 2;
-        J_.done = done_; J_.errKeys = errKeys_; J_.retries = retries_; J_.range = rangeOf_;
+        J_.done = done_; J_.errKeys = errKeys_; J_.retries = retries_; J_.slot = slotOf_;
         J_.refillMin = static_cast<uint32_t>(cfg_.pool * cfg_.refillPercent / 100);
         J_.ring = q_.free[1];
         J_.head = ctl_ + 4;
@@ -471,12 +472,23 @@ class Engine {
             Active& a = *best;
             uint64_t n = std::min<uint64_t>(cfg_.rangeSamples, a.total - a.issued);
             if (a.frameSamples) n = std::min<uint64_t>(n, (a.issued / a.frameSamples + 1) * a.frameSamples - a.issued);
-            // whole samples of every pixel where a range holds at least one: issued pixel-major,
-            // so a warp's paths start samples of one pixel (as in a single render's chunks)
-            uint32_t spp = 0;
-            if (a.pixels <= n && a.issued % a.pixels == 0) {
+            // Ranges are issued pixel-major, so a warp's paths start samples of one pixel (as in a
+            // single render's chunks). A job without progressive frames whose samples per pixel
+            // fit a range is cut into blocks of pixels that each range holds every sample of (a
+            // warp: min(32, spp) samples of one pixel); otherwise into whole samples of every
+            // pixel where a range holds at least one.
+            uint32_t spp = 0, s0 = 0, p0 = 0;
+            const uint64_t perPixel = a.total / a.pixels;
+            if (!a.frameSamples && perPixel <= cfg_.rangeSamples && a.pixels <= UINT32_MAX && a.issued % perPixel == 0) {
+                const uint64_t first = a.issued / perPixel;
+                const uint64_t count = std::min<uint64_t>(std::max<uint64_t>(1, cfg_.rangeSamples / perPixel), a.pixels - first);
+                n = count * perPixel;
+                spp = static_cast<uint32_t>(perPixel);
+                p0 = static_cast<uint32_t>(first);
+            } else if (a.pixels <= n && a.issued % a.pixels == 0) {
                 n = n / a.pixels * a.pixels;
                 spp = static_cast<uint32_t>(n / a.pixels);
+                s0 = static_cast<uint32_t>(a.issued / a.pixels);
             }
             uint64_t at = 0;
             if (!arena_.take(n, at)) return;
@@ -488,8 +500,8 @@ class Engine {
             R.pixels = a.pixels;
             R.job = a.slot;
             R.spp = spp;
-            R.s0 = spp ? static_cast<uint32_t>(a.issued / a.pixels) : 0;
-            R.pad = 0;
+            R.s0 = s0;
+            R.p0 = p0;
             a.ranges.push_back(rangeCount_);
             closed_.push_back(false);
             ++a.chunks;
@@ -743,7 +755,7 @@ class Engine {
     DevAlloc pool_, scratchAlloc_;
     PathSoA st_{}, one_{};
     Queues q_{}, oneQ_{};
-    uint32_t* rangeOf_ = nullptr;
+    uint2* slotOf_ = nullptr;
     unsigned long long* stats_ = nullptr;
     DevScene* scenes_ = nullptr;
     RenderParams* params_ = nullptr;

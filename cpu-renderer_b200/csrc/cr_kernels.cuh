@@ -25,10 +25,12 @@ namespace crg {
 // position j starts sample s0 + j % spp of pixel j / spp, so the consecutive path slots that
 // form a warp start samples of one pixel and trace nearly the same rays for longer (a smooth
 // dielectric or a mirror sends them the same way). Either order, each pixel's samples are
-// summed in sample order, so the film does not depend on it.
+// summed in sample order, so the film does not depend on it. A pixel-major chunk may also
+// cover a block of pixels only, [p0, p0 + (c1 - c0) / spp): then it holds every sample of them.
 struct Chunk {
     uint64_t c0, c1, pixels;
     uint32_t spp = 0, s0 = 0;  // spp 0: sample-major positions
+    uint32_t p0 = 0;           // pixel-major: the first pixel
 };
 
 // Where a path's sample radiance goes: out[base + sample * sampleStride + pixel * pixelStride].
@@ -36,7 +38,7 @@ struct OutRef {
     uint64_t base, sampleStride, pixelStride;
 };
 CR_D OutRef outOf(const Chunk& C) {
-    if (C.spp) return OutRef{0ull - C.s0, 1, C.spp};
+    if (C.spp) return OutRef{0ull - C.s0 - static_cast<uint64_t>(C.p0) * C.spp, 1, C.spp};
     return OutRef{0ull - C.c0, C.pixels, 1};
 }
 // out[] index of a pixel's sample
@@ -47,7 +49,7 @@ CR_D uint64_t outIndex(const OutRef& O, uint32_t pixel, uint32_t sample) {
 // The pixel and sample that position j of the chunk starts.
 CR_D void chunkSample(const Chunk& C, uint64_t j, uint32_t& pixel, uint32_t& sample) {
     if (C.spp) {
-        pixel = static_cast<uint32_t>(j / C.spp);
+        pixel = C.p0 + static_cast<uint32_t>(j / C.spp);
         sample = C.s0 + static_cast<uint32_t>(j % C.spp);
     } else {
         const uint64_t id = C.c0 + j;
@@ -67,15 +69,16 @@ struct IssueRange {
     uint64_t outBase;  // out[] index of the range's first position
     uint64_t pixels;   // the job's width * height
     uint32_t job;      // job slot
-    uint32_t spp;      // > 0: whole samples [s0, s0 + spp) of every pixel, issued pixel-major (see Chunk)
+    uint32_t spp;      // > 0: samples [s0, s0 + spp) of every pixel from p0 on, issued pixel-major (see Chunk)
     uint32_t s0;
-    uint32_t pad;
+    uint32_t p0;
 };
 // The range as a chunk (its positions map to pixels and samples the same way).
 CR_HD Chunk rangeChunk(const IssueRange& R) {
     Chunk C{R.c0, R.c1, R.pixels};
     C.spp = R.spp;
     C.s0 = R.s0;
+    C.p0 = R.p0;
     return C;
 }
 struct JobTable {
@@ -87,7 +90,8 @@ struct JobTable {
     unsigned long long* done;        // [range] finished samples
     unsigned long long* errKeys;     // [job slot] smallest error key
     unsigned long long* retries;     // [job slot] precision replays
-    uint32_t* range;                 // [path slot] the path's range
+    uint2* slot;                     // [path slot] the path's range (x) and job slot (y), one
+                                     // load ahead of its scene's fields
     uint32_t refillMin;              // refill only when at least this many slots are free
     // The pool's free slots, a ring over `ring` (capacity `poolSize`): k_regen claims from the
     // head (ping-pong by iteration parity, so every block of a launch reads the same head),
@@ -564,18 +568,20 @@ struct PathJob {
     unsigned long long* retries;
     uint32_t r;
 };
-CR_D PathJob pathJob(const JobTable& J, uint32_t path) {
-    const uint32_t r = J.range[path];
+CR_D PathJob pathJob(const JobTable& J, uint2 sj) {
+    const uint32_t r = sj.x, job = sj.y;
     const IssueRange& R = J.ranges[r];
     PathJob pj;
-    pj.S = J.scenes + R.job;
-    pj.P = J.params + R.job;
-    pj.O = R.spp ? OutRef{R.outBase - R.s0, 1, R.spp} : OutRef{R.outBase - R.c0, R.pixels, 1};
-    pj.E = ErrSink{J.errKeys + R.job, nullptr};
-    pj.retries = J.retries + R.job;
+    pj.S = J.scenes + job;
+    pj.P = J.params + job;
+    pj.O = R.spp ? OutRef{R.outBase - R.s0 - static_cast<uint64_t>(R.p0) * R.spp, 1, R.spp}
+                 : OutRef{R.outBase - R.c0, R.pixels, 1};
+    pj.E = ErrSink{J.errKeys + job, nullptr};
+    pj.retries = J.retries + job;
     pj.r = r;
     return pj;
 }
+CR_D PathJob pathJob(const JobTable& J, uint32_t path) { return pathJob(J, J.slot[path]); }
 // The range holding issue position pos (the last range starting at or before it).
 CR_D uint32_t findRange(const JobTable& J, uint32_t count, uint64_t pos) {
     uint32_t lo = 0, hi = count;  // ranges[lo].start <= pos < ranges[hi].start
@@ -665,7 +671,7 @@ __global__ void __launch_bounds__(128) k_regen(DevScene S, RenderParams P, PathS
                 const uint64_t j = pos - R.start;
                 uint32_t pixel, sample;
                 chunkSample(rangeChunk(R), j, pixel, sample);
-                J.range[slot] = r;
+                J.slot[slot] = make_uint2(r, R.job);
                 const ErrSink Ej{J.errKeys + R.job, nullptr};
                 live = initPath(J.scenes[R.job], J.params[R.job], st, slot, pixel, sample, false, Ej);
                 if (!live) {  // the sample is done (radiance 0); k_trace returns the slot to the ring
@@ -708,10 +714,11 @@ __global__ void __launch_bounds__(BLOCK, CR_TRACE_MIN_BLOCKS * 128 / BLOCK) k_tr
         if (idx < nE) {
             path = q.extend[cur][idx];
             if constexpr (MULTI) {
+                const uint2 sj = J.slot[path];  // loaded beside the flags, not after them
                 if (st.flags[path] == kPathNull) {
                     freed = true;  // a sample whose camera ray failed: only its slot comes back
                 } else {
-                    const PathJob pj = pathJob(J, path);
+                    const PathJob pj = pathJob(J, sj);
                     cls = closestOne<COUNT, NOALPHA>(*pj.S, *pj.P, st, path, pj.E, stats);
                 }
             } else {
@@ -774,15 +781,17 @@ __global__ void __launch_bounds__(BLOCK, CR_SHADE_MIN_BLOCKS * 128 / BLOCK) k_sh
 // render.cpp:390-413: each pixel adds the chunk's samples in index order.
 static __global__ void k_accumulate(const float4* out, Chunk C, double* acc) {
     if (C.spp) {  // pixel-major chunk: a pixel's samples are consecutive
-        for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < C.pixels;
+        const uint64_t count = (C.c1 - C.c0) / C.spp;  // pixels from p0 on
+        for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < count;
              p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-            double r = acc[3 * p], g = acc[3 * p + 1], b = acc[3 * p + 2];
+            double* a = acc + 3 * (C.p0 + p);
+            double r = a[0], g = a[1], b = a[2];
             const float4* o = out + p * C.spp;
             for (uint32_t k = 0; k < C.spp; ++k) {
                 const float4 v = o[k];
                 r += v.x; g += v.y; b += v.z;
             }
-            acc[3 * p] = r; acc[3 * p + 1] = g; acc[3 * p + 2] = b;
+            a[0] = r; a[1] = g; a[2] = b;
         }
         return;
     }

@@ -80,6 +80,24 @@ def test_batch_films_equal_single_renders(crgpu, world, tuning):
         assert stats["graph_steps"] > 0
 
 
+@pytest.mark.parametrize("range_samples", [1024, 1600, 6000])
+def test_batch_range_shapes(crgpu, world, range_samples):
+    """A job whose samples per pixel fit a range is issued as blocks of pixels holding all their
+    samples; one whose samples per pixel exceed it (1536 spp against 1024) as slices of whole
+    samples of every pixel. Either shape, and a last block or slice cut short, sums every pixel
+    in sample order: films equal the single renders'."""
+    jobs = [JobSpec(world["room"], world["room_cam"], _opts(crgpu, 8, 6, 1536, bounces=4)),
+            JobSpec(world["grid"], world["grid_cam"], _opts(crgpu, 33, 17, 48, seed=9)),
+            JobSpec(world["room"], world["room_cam"], _opts(crgpu, 7, 5, 1, seed=3))]
+    stats = render_batch(jobs, EngineTuning.make(pool_paths=4096, range_samples=range_samples, solo_samples_log2=64))
+    assert stats["jobs_done"] == len(jobs) and stats["jobs_failed"] == 0
+    for i, j in enumerate(jobs):
+        assert j.status == 0, j.error
+        film, st = _alone(j)
+        assert np.array_equal(j.film, film), f"job {i}"
+        assert j.stats["camera_samples"] == st["camera_samples"]
+
+
 def test_batch_solo_jobs(crgpu, world):
     """Jobs of at least 2^solo_samples_log2 samples between two drains render alone through the
     single-render path (here 2^14: the 64x48x16, 160x90x4 and 128x128x2 jobs, and the

@@ -9,7 +9,8 @@
 // Minimum resident blocks per SM requested from the register allocator (128-thread blocks).
 // k_trace at 12 (40 registers, some spills to L1) measured ~2 % faster than at 8 or 10 on
 // the 1M-triangle workload; k_shade above 4 loses more to spills than it gains (also per
-// class: the NEE-null kernel at 5, 6 or 8 and the miss kernel at 8 measured slower).
+// class: the miss kernel at 8 measured slower; the NEE-null kernel, at 110 registers since it
+// samples only the BSDF's delta branches, measured the same at 5 and 6 as at 4).
 #ifndef CR_TRACE_MIN_BLOCKS
 #define CR_TRACE_MIN_BLOCKS 12
 #endif
@@ -217,8 +218,9 @@ CR_D void finishPath(const RenderParams& P, const OutRef& O, const PathSoA& st, 
 // closest hit is known. cont: the path continues; shadow: a shadow ray was queued (a path
 // that ends with a queued shadow ray is finished by k_trace next iteration); freed: the path
 // ended and its slot can take a new sample. CLASS specialises the code: kShadeMiss holds only
-// environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces, kShadeConductor only
-// hits on kTriConductor surfaces (the BSDF without its zero lobes), kShadeGeneric anything.
+// environment misses, kShadeNeeNull only hits on kTriNeeNull surfaces (the BSDF's delta
+// branches alone), kShadeConductor only hits on kTriConductor surfaces (the BSDF without its
+// zero lobes), kShadeGeneric anything.
 template <int CLASS, bool GUIDED = false, bool LEAN = false>
 CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, const PathSoA& st, uint32_t path,
                    const ErrSink& E, unsigned long long* retries, bool& cont, bool& shadow, bool& freed) {
@@ -373,6 +375,8 @@ CR_D void shadeOne(const DevScene& S, const RenderParams& P, const OutRef& O, co
         }
     } else if constexpr (CLASS == kShadeConductor) {
         smp = sampleConductor(s, wo, rng);  // render.cpp:302-303
+    } else if constexpr (CLASS == kShadeNeeNull) {
+        smp = sampleSmooth(s, wo, rng);  // render.cpp:302-303 (the BSDF's delta branches)
     } else {
         smp = sampleBsdf(s, wo, rng);  // render.cpp:302-303
     }

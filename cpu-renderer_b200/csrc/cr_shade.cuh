@@ -354,6 +354,45 @@ CR_D BsdfSample sampleBsdf(const Surface& s, V3 wo, Rng& rng) {
     return out;
 }
 
+// sampleBsdf for a kTriNeeNull surface: smooth (roughness <= 0.001 with no texture that could
+// change it), and metallic exactly 1 or transmission exactly 1 (no texture that could change
+// it). Its diffuse weight (1 - metallic) * (1 - transmission) * ... is then 0 (or NaN, which
+// leaves the total not above 0 and every probability 0), so the diffuse lobe is never drawn,
+// and the microfacet lobe is smooth, so it returns its delta sample before any evaluation.
+// What remains is sampleBsdf's own arithmetic on those two branches, drawing the same numbers
+// (u and v of the microfacet lobe are drawn and unused, as there).
+CR_D BsdfSample sampleSmooth(const Surface& s, V3 wo, Rng& rng) {
+    const Ctx c(s, wo);
+    BsdfSample out = emptySample();
+    if (c.wo.z <= 1e-7f) return out;
+    const float lobe = rng.uniform();
+    if (lobe < c.diffuseProbability + c.deltaTransmissionProbability) {
+        out.direction = -wo; out.delta = true; out.transmitted = true; out.pdf = c.deltaTransmissionProbability;
+        out.weight = s.baseColor * ((1 - s.metallic) * s.transmission / out.pdf);
+        return correctGeometricSide(s, wo, out.direction, true) ? out : emptySample();
+    }
+    rng.uniform();
+    rng.uniform();
+    const V3 h{0, 0, 1};
+    const float oh = dot(c.wo, h), f = c.fresnel(oh), pr = c.reflectionProbability(f, oh);
+    const bool reflection = rng.uniform() < pr;
+    V3 wi;
+    if (reflection) wi = reflect(-c.wo, h);
+    else if (c.thin) wi = -c.wo;
+    else if (!refractDirection(c.wo, h, 1 / c.eta, wi)) return out;
+    if ((reflection && wi.z <= 0) || (!reflection && wi.z >= 0)) return out;
+    out.transmitted = !reflection;
+    out.eta = out.transmitted && !c.thin ? c.eta : 1;
+    out.delta = true;
+    out.direction = normalize(c.frame.world(wi));
+    if (!correctGeometricSide(s, wo, out.direction, out.transmitted)) return emptySample();
+    const float prob = c.microProbability() * (reflection ? pr : 1 - pr);
+    if (prob <= 0) return emptySample();
+    out.pdf = prob;
+    out.weight = (reflection ? c.reflection(f, oh) : c.transmission(f) / (out.eta * out.eta)) / prob;
+    return out;
+}
+
 // ---- GGX conductor (the bsdf.cpp BSDF at metallic exactly 1, transmission exactly 0) -----------
 // A material with metallic 1, transmission 0 and no texture that could change either (the
 // kTriConductor surfaces) has, in the BSDF above: diffuse and transmission weights

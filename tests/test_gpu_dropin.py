@@ -1,6 +1,7 @@
 """Drop-in check: the reference's own integrator and transport-edge test suites
 (tests/test_integrator.cpp, tests/test_transport_edges.cpp), compiled from its sources with
-cpu-renderer_b200/host/render_gpu.cpp in place of src/render.cpp, pass on the GPU backend.
+cr::render defined by cpu-renderer_b200/host/render_gpu.cpp (src/render.cpp compiled with
+that function renamed, so cr::Environment is the reference's own), pass on the GPU backend.
 The binaries are built by `make -f oracle/Makefile dropin` where the reference sources are
 present and travel with the build tree."""
 import os

@@ -52,6 +52,7 @@ def _load():
                                                C.POINTER(C.c_uint64)]),
         "cr_gpu_render_noalloc": (C.c_int, [P, C.POINTER(Camera), C.POINTER(Options), P, C.POINTER(Stats)]),
         "cr_gpu_allocation_count": (C.c_int, [C.POINTER(C.c_uint64)]),
+        "cr_gpu_debug_fail_allocation": (C.c_int, [C.c_int64]),
         "cr_display_thresholds": (C.c_int, [C.c_float, P]),
         "cr_gpu_film_encode": (C.c_int, [P, C.c_int, C.c_float, P, C.c_uint64, C.POINTER(C.c_uint64)]),
         "cr_gpu_encode": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, P, C.c_uint64, C.POINTER(C.c_uint64)]),
@@ -110,6 +111,12 @@ def allocation_count():
     n = C.c_uint64(0)
     check(lib.cr_gpu_allocation_count(C.byref(n)))
     return n.value
+
+
+def fail_allocation(nth):
+    """Test hook: the nth device allocation from now (0: the next) fails as out of memory;
+    a negative nth disarms it."""
+    check(lib.cr_gpu_debug_fail_allocation(int(nth)))
 
 
 def device_count():

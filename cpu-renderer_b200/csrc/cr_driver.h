@@ -129,6 +129,7 @@ struct DevAlloc {
         int device = 0;
         CR_CUDA(cudaGetDevice(&device));
         crh::count_allocation();
+        if (crh::injected_allocation_failure()) throw CudaError(cudaErrorMemoryAllocation, "device allocation (injected failure)");
         auto [p, have] = BlockCache::get().take(device, want);
         if (!p) {
             if (cudaMalloc(&p, want) != cudaSuccess) {
@@ -223,7 +224,12 @@ struct cr_gpu_scene {
         if (pixels <= filmPixels) return;
         CR_CUDA(cudaStreamSynchronize(stream));
         filmAlloc.release();
+        // The last film went back with its blocks (a failed allocation below may even hand them
+        // to the driver): until a render completes in the new ones there is no film to read.
+        acc = nullptr;
+        film = nullptr;
         filmPixels = 0;
+        filmWidth = filmHeight = 0;
         acc = filmAlloc.alloc<double>(3 * pixels);
         film = filmAlloc.alloc<float>(3 * pixels);
         filmPixels = pixels;

@@ -235,13 +235,16 @@ uint64_t encode_film(const float* dFilm, int width, int height, int format, floa
     EncodeCache& E = cacheFor(device);
     std::lock_guard<std::mutex> lock(E.encodeMutex);
     if (!E.check) {
+        // E.check is set last: until every buffer exists the next call sets them up again
         for (int k = 0; k < 3; ++k) crh::count_allocation();
-        ENC_CUDA(cudaMalloc(&E.check, sizeof(Check)));
-        ENC_CUDA(cudaMalloc(&E.thresholds, 256 * sizeof(float)));
-        ENC_CUDA(cudaMallocHost(&E.hostCheck, sizeof(Check)));
+        if (!E.thresholds) ENC_CUDA(cudaMalloc(&E.thresholds, 256 * sizeof(float)));
+        if (!E.hostCheck) ENC_CUDA(cudaMallocHost(&E.hostCheck, sizeof(Check)));
         int sms = 0;
         ENC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         E.grid = sms * 8;
+        Check* check = nullptr;
+        ENC_CUDA(cudaMalloc(&check, sizeof(Check)));
+        E.check = check;
     }
     const Check init{kNone, kNone, 0};
     ENC_CUDA(cudaMemcpyAsync(E.check, &init, sizeof(Check), cudaMemcpyHostToDevice, s));

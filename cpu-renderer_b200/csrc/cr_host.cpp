@@ -244,9 +244,17 @@ const std::string& last_error_text() { return g_lastError; }
 
 namespace {
 std::atomic<uint64_t> g_allocations{0};
+std::atomic<int64_t> g_failCountdown{-1};  // allocations left before the injected failure; -1: none
 }
 void count_allocation() { g_allocations.fetch_add(1, std::memory_order_relaxed); }
 uint64_t allocation_count() { return g_allocations.load(std::memory_order_relaxed); }
+void inject_allocation_failure(int64_t nth) { g_failCountdown.store(nth < 0 ? -1 : nth, std::memory_order_relaxed); }
+bool injected_allocation_failure() {
+    int64_t v = g_failCountdown.load(std::memory_order_relaxed);
+    while (v >= 0 && !g_failCountdown.compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) {
+    }
+    return v == 0;
+}
 
 void validate_options(const cr_render_options& o) {
     if (o.width < 1 || o.height < 1 || o.width > 16384 || o.height > 16384)

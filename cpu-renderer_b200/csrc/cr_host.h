@@ -25,6 +25,10 @@ const std::string& last_error_text();  // this thread's last message
 // site calls count_allocation(); cr_gpu_allocation_count reports the total.
 void count_allocation();
 uint64_t allocation_count();
+// Fault injection for tests: the nth device allocation from now (0: the next) made through
+// crd::DevAlloc fails as if the device were out of memory; a negative nth disarms it.
+void inject_allocation_failure(int64_t nth);
+bool injected_allocation_failure();  // consumes one allocation of the countdown
 
 void validate_options(const cr_render_options& o);                           // render.cpp:97-104
 

@@ -587,10 +587,15 @@ struct GuideRun {
 void ensureAlias(cr_gpu_scene& g) {
     if (!g.dev.env_has_image || g.dev.alias_threshold) return;
     crh::build_alias(g.env);
-    g.dev.alias_threshold = reinterpret_cast<const unsigned long long*>(
+    // The scene takes the tables only once all three exist: a failed upload leaves it without
+    // them (and the next request builds them again), never with some of them.
+    const auto* threshold = reinterpret_cast<const unsigned long long*>(
         g.aliasAlloc.upload(g.env.aliasThreshold.data(), g.env.aliasThreshold.size(), g.stream));
-    g.dev.alias_index = g.aliasAlloc.upload(g.env.aliasIndex.data(), g.env.aliasIndex.size(), g.stream);
-    g.aliasPdf = g.aliasAlloc.upload(g.env.aliasPdf.data(), g.env.aliasPdf.size(), g.stream);
+    const auto* index = g.aliasAlloc.upload(g.env.aliasIndex.data(), g.env.aliasIndex.size(), g.stream);
+    const float* pdf = g.aliasAlloc.upload(g.env.aliasPdf.data(), g.env.aliasPdf.size(), g.stream);
+    g.dev.alias_index = index;
+    g.aliasPdf = pdf;
+    g.dev.alias_threshold = threshold;
 }
 
 // The whole render. filmHost may be NULL (film stays on the device).
@@ -1177,6 +1182,11 @@ extern "C" {
 cr_status cr_gpu_allocation_count(uint64_t* count) {
     if (!count) return crh::set_last_error(CR_ERR_INVALID_ARGUMENT, "count is NULL");
     *count = crh::allocation_count();
+    return CR_OK;
+}
+
+cr_status cr_gpu_debug_fail_allocation(int64_t nth) {
+    crh::inject_allocation_failure(nth);
     return CR_OK;
 }
 

@@ -360,6 +360,17 @@ cr_status cr_gpu_render_noalloc(cr_gpu_scene* scene, const cr_camera* camera,
  * page-locked host blocks alike. A call that allocates nothing leaves it unchanged. */
 cr_status cr_gpu_allocation_count(uint64_t* count);
 
+/* Fault injection for tests (no counterpart in the reference, which has none): the nth device
+ * allocation from now (0: the next one) that goes through the library's device allocator fails
+ * as if the device were out of memory, and the call that made it returns CR_ERR_OUT_OF_MEMORY
+ * with "device allocation (injected failure)" in its message; a negative nth disarms it. That
+ * allocator holds scenes (geometry, sky, alias tables), render workspaces, films, guided-render
+ * buffers and the engine's job buffers; the encoder's buffers and page-locked staging do not go
+ * through it. Process-wide: allocations made on other threads count too. A failed call leaves
+ * every object usable: the same call made again after disarming returns what it would have
+ * returned without the failure. */
+cr_status cr_gpu_debug_fail_allocation(int64_t nth);
+
 /* ---- output encoding on the device ----------------------------------------------------------
  * Replaces the per-pixel work of io::writePng / io::writeHdr (src/io/image.cpp:100-124,
  * 193-230; scene.h:144-146), which the reference runs on the CPU after cr::render.

@@ -135,6 +135,17 @@ class Engine {
   public:
     Engine(int device, const cr_engine_tuning* tuning, int defaultPolicy)
         : device_(device), cfg_(makeConfig(tuning, defaultPolicy)), arena_(0) {
+        try {
+            setUp();
+        } catch (...) {
+            releaseAll();  // a constructor that throws runs no destructor
+            throw;
+        }
+    }
+    ~Engine() { releaseAll(); }
+
+  private:
+    void setUp() {
         CR_CUDA(cudaSetDevice(device_));
         CR_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
         start_ = std::chrono::steady_clock::now();
@@ -199,7 +210,8 @@ class Engine {
         J_.poolSize = cfg_.pool;
     }
 
-    ~Engine() {
+    // Everything the engine holds; also what a failed set-up had taken so far.
+    void releaseAll() {
         cudaSetDevice(device_);
         if (s_) cudaStreamSynchronize(s_);
         for (auto& g : graph_) if (g) cudaGraphExecDestroy(g);
@@ -214,6 +226,7 @@ class Engine {
         if (s_) cudaStreamDestroy(s_);
     }
 
+  public:
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - start_).count(); }
 
     uint64_t submit(cr_job* j) {

@@ -484,6 +484,8 @@ struct cr_guide {
     void* ensureScratch(size_t bytes) {
         if (bytes > scratchBytes) {
             scratch.release();
+            scratchPtr = nullptr;  // until the larger block exists (its allocation may fail)
+            scratchBytes = 0;
             scratchPtr = scratch.alloc<unsigned char>(bytes);
             scratchBytes = bytes;
         }

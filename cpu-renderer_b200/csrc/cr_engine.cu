@@ -299,8 +299,16 @@ class Engine {
             for (auto& p : pending_) victims.push_back(p);
             pending_.clear();
         }
-        for (auto& a : active_) victims.push_back({a.job, a.ticket});
+        // the jobs' buffers go back once nothing queued can still write them (after a CUDA
+        // error the wait returns at once)
+        if (s_) cudaStreamSynchronize(s_);
+        cudaGetLastError();
+        for (auto& a : active_) {
+            victims.push_back({a.job, a.ticket});
+            a.buffers.release();
+        }
         active_.clear();
+        usedBytes_ = 0;
         for (auto& v : victims) endJob(v.first, v.second, status, message);
     }
 

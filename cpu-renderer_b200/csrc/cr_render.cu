@@ -100,12 +100,25 @@ struct Workspace {
     cudaStream_t side[kSide] = {nullptr, nullptr, nullptr};
     cudaEvent_t fork = nullptr, join[kSide] = {nullptr, nullptr, nullptr};
 
+    // Each handle is taken only once it exists, so a creation that fails part-way is completed
+    // by the next call instead of leaving a null stream (the legacy default stream) or event.
     void ensureSideStreams() {
-        if (side[0]) return;
-        CR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        if (!fork) {
+            cudaEvent_t e = nullptr;
+            CR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            fork = e;
+        }
         for (int k = 0; k < kSide; ++k) {
-            CR_CUDA(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
-            CR_CUDA(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming));
+            if (!side[k]) {
+                cudaStream_t st = nullptr;
+                CR_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                side[k] = st;
+            }
+            if (!join[k]) {
+                cudaEvent_t e = nullptr;
+                CR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                join[k] = e;
+            }
         }
     }
 
